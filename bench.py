@@ -1,0 +1,489 @@
+#!/usr/bin/env python
+"""Benchmark of the Merbit merge-path CSR SpMV on B200.
+
+Workload (default): the power-law matrix -- 2,000,000 x 2,000,000, row
+lengths Zipf(1.8) capped at 200,000, 10% empty rows, sorted unique uniform
+columns, values N(0,1), x ~ U[-1,1], seed 1 -- in plain FP64 (values, x, y
+and accumulation).  It stands in for the reference harness's Matrix Market
+graphs, which are not available; the generator is merbit_b200/synth.py.
+
+One step = one SpMV  y = A x  over the resident matrix (the reference's
+harness times the same unit: tim2 / 400, include/tile.cuh:599-608).
+
+  value  GB/s of algorithmic traffic, B = 4(nrow+1) + nnz(4+8) + 8 ncol + 8 nrow,
+         over K back-to-back steps timed with CUDA events on the launching
+         stream; the matrix (~0.6 GB) is larger than L2, so each step streams
+         it from HBM (x, 16 MB, may stay in L2 between steps).
+  e2e    the same metric through the public API (merbit_b200.Plan.spmv) with
+         host buffers: every step copies x from pinned host memory, runs the
+         SpMV and copies y back.
+  roofline  the SpMV kernel's algorithmic bytes / its mean launch time vs the
+         measured HBM copy bandwidth (MEASURED_PEAKS.json).
+  cpu_baseline  the merge-path OpenMP FP64 SpMV of the CPU oracle on all host
+         cores (the reference ships no CPU SpMV; this is its restatement).
+
+Multi-GPU (torchrun): each rank runs its own copy of the workload (weak
+scaling, no data-path collective); value = all ranks' bytes / the slowest
+rank's time.
+
+--impl reference times the CPU restatement on this host's cores as the
+reference arm, and the reference's own merbit_kernel (built from the
+reference sources into oracle/_ref) on the GPU as an extra field.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "SpMV GB/s (% of HBM peak) & GFLOP/s; mixed/batched vs plain FP64 at 1e-6 rel"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="zipf_2m")
+    ap.add_argument("--dtype", choices=["f64", "f32", "bf16"], default="f64")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def alg_bytes(A, dtype: str, k: int = 1) -> float:
+    sv = {"f64": 8, "f32": 4, "bf16": 2}[dtype]
+    sxy = 8 if dtype == "f64" else 4
+    return 4.0 * (A.nrow + 1) + A.nnz * (4.0 + sv) + k * sxy * (A.ncol + A.nrow)
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+        0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+        0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+        0x100: "display_clock_setting",
+    }
+
+    def __init__(self, index: int, period_s: float = 0.005):
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._ok = False
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._ok = True
+        except Exception:
+            self._ok = False
+        self.period = period_s
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                self.samples.append((mhz, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def start(self):
+        if self._ok:
+            self._t.start()
+        return self
+
+    def stop(self):
+        self._stop.set()
+        if self._ok:
+            self._t.join()
+        return self
+
+    def summary(self):
+        if not self._ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml_unavailable"],
+                    "samples": 0}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        mhz = [m for m, _ in self.samples]
+        bits = 0
+        for _, r in self.samples:
+            bits |= r
+        reasons = [n for b, n in self.REASONS.items() if bits & b and n != "gpu_idle"]
+        return {"sm_mhz": float(statistics.median(mhz)), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(mhz)}
+
+
+def dist_setup(args):
+    import torch
+
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def allreduce_max(ws, v: float) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def load(args):
+    from merbit_b200 import synth
+
+    A = synth.workload(args.workload)
+    x = synth.uniform(1, A.ncol)
+    return A, x
+
+
+def cpu_baseline(A, x, seconds: float):
+    """Timed OpenMP FP64 merge-path SpMV (oracle/, CPU restatement)."""
+    from oracle import oracle as O
+
+    y = np.empty(A.nrow)
+    vals = np.ascontiguousarray(A.vals, np.float64)
+    O.spmv_omp_f64(A.row_ptr, A.col, vals, x, y)  # warm-up (page-in, thread spin-up)
+    times = []
+    t_end = time.perf_counter() + seconds
+    threads = 1
+    while time.perf_counter() < t_end or len(times) < 3:
+        t0 = time.perf_counter()
+        _, threads = O.spmv_omp_f64(A.row_ptr, A.col, vals, x, y)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= 200:
+            break
+    med = statistics.median(times)
+    return y, med, threads, len(times)
+
+
+def traffic_from_profile(workload: str, dtype: str):
+    p = os.path.join(ROOT, "profiles", f"spmv_{dtype}_{workload}_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+def run_ours(args):
+    import torch
+
+    import merbit_b200 as mb
+
+    ws, rank, local = dist_setup(args)
+    A, x = load(args)
+    dev = torch.device("cuda", local)
+    vt = {"f64": torch.float64, "f32": torch.float32, "bf16": torch.bfloat16}[args.dtype]
+    xt = torch.float64 if args.dtype == "f64" else torch.float32
+    rp = torch.from_numpy(A.row_ptr).to(dev)
+    col = torch.from_numpy(A.col).to(dev)
+    vals = torch.from_numpy(A.vals).to(dev).to(vt)
+    xd = torch.from_numpy(x).to(dev).to(xt)
+    yd = torch.empty(A.nrow, dtype=xt, device=dev)
+    plan = mb.Plan(rp, col, vals, ncol=A.ncol)
+    if not args.no_tune:
+        plan.tune(xd)
+    info = plan.info()
+    B = alg_bytes(A, args.dtype)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(max(args.warmup, 3)):
+        plan.spmv(xd, yd)
+    torch.cuda.synchronize(dev)
+
+    # ---- timed region: K back-to-back steps
+    sampler = ClockSampler(local).start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.spmv(xd, yd)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    sampler.stop()
+    ms_local = e0.elapsed_time(e1) / args.steps
+    ms = allreduce_max(ws, ms_local)
+    plan.check()
+
+    # ---- per-launch duration of the SpMV kernel with L2 flushed before each
+    # launch (cold x as well as cold matrix)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    nflush = min(args.steps, 50)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(nflush)]
+    for a, b in evs:
+        flush.fill_(1)
+        a.record(stream)
+        plan.spmv(xd, yd)
+        b.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_cold = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    del flush
+
+    # ---- e2e through the public API with host buffers
+    xh = torch.from_numpy(x).to(xt).pin_memory()
+    yh = torch.empty(A.nrow, dtype=xt).pin_memory()
+    ke = min(args.steps, 200)
+    for _ in range(3):
+        xd.copy_(xh, non_blocking=True)
+        plan.spmv(xd, yd)
+        yh.copy_(yd, non_blocking=True)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(ke):
+        xd.copy_(xh, non_blocking=True)
+        plan.spmv(xd, yd)
+        yh.copy_(yd, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    ms_e2e = allreduce_max(ws, e0.elapsed_time(e1) / ke)
+    y_gpu = yh.numpy().astype(np.float64)
+
+    if rank != 0:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+
+    peak, peak_src = peaks()
+    value = ws * B / (ms * 1e-3) / 1e9
+    achieved = B / (ms * 1e-3) / 1e9
+    traffic = traffic_from_profile(args.workload, args.dtype)
+    out = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": max(args.warmup, 3),
+        "ms_per_step": round(ms, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": args.dtype,
+        "data": "synthetic (seeded generator merbit_b200/synth.py; the reference's "
+                "Matrix Market graphs are not available)",
+        "config": {
+            "workload": args.workload,
+            "nrow": A.nrow, "ncol": A.ncol, "nnz": A.nnz,
+            "values": args.dtype, "k": 1,
+            "l2": "inputs larger than L2 (matrix streamed from HBM every step); "
+                  "value_l2_flushed flushes L2 before every launch",
+            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+            "kernel": f"spmv_tile_kernel block={info.block} ipt={info.items_per_thread} "
+                      f"tile_items={info.tile_items} tiles={info.num_tiles} "
+                      f"vectorized={int(info.vectorized)}",
+        },
+        "pct_hbm_peak": round(100.0 * achieved / peak, 2),
+        "gflops": round(ws * 2.0 * A.nnz / (ms * 1e-3) / 1e9, 2),
+        "value_l2_flushed": round(ws * B / (ms_cold * 1e-3) / 1e9, 2),
+        "algorithmic_bytes_per_step": B,
+        "plan_metadata_bytes": info.metadata_bytes,
+        "gpu_launches": args.steps,
+        "roofline": {
+            "bound": "hbm",
+            "achieved": round(achieved, 2),
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "peak_source": f"{peak_src} hbm_gbs (copy), burst",
+            "traffic": traffic,
+            "kernel": "spmv_tile_kernel",
+        },
+        "e2e": {
+            "value": round(ws * B / (ms_e2e * 1e-3) / 1e9, 2),
+            "unit": "GB/s",
+            "h2d_bytes_per_step": int(xh.numel() * xh.element_size()),
+            "d2h_bytes_per_step": int(yh.numel() * yh.element_size()),
+            "ms_per_step": round(ms_e2e, 5),
+            "api": "merbit_b200.Plan.spmv (C ABI merbit_spmv)",
+        },
+        "clocks": sampler.summary(),
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        y_cpu, t_cpu, threads, reps = cpu_baseline(A, x, args.cpu_seconds)
+        out["cpu_baseline"] = {
+            "value": round(B / t_cpu / 1e9, 3),
+            "unit": "GB/s",
+            "cores": threads,
+            "kind": "port",
+            "sample": f"full {args.workload} matrix, FP64, median of {reps} SpMVs "
+                      f"(merge-path OpenMP restatement in oracle/merbit_oracle.c)",
+        }
+        # component-wise error |y - y_cpu| / sum_j |a_ij x_j|
+        rows = np.repeat(np.arange(A.nrow), np.diff(A.row_ptr))
+        yabs = np.bincount(rows, weights=np.abs(A.vals) * np.abs(x[A.col]), minlength=A.nrow)
+        rel = np.abs(y_gpu - y_cpu) / np.maximum(yabs, 1e-300)
+        out["err_vs_cpu_fp64"] = {"max": float(rel.max()), "median": float(np.median(rel)),
+                                  "note": "component-wise, vs the FP64 CPU baseline's y"}
+    print(json.dumps(out), flush=True)
+
+
+def run_reference(args):
+    import torch
+
+    ws, rank, local = dist_setup(args)
+    if rank != 0:
+        barrier(ws)
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    from oracle import oracle as O
+
+    A, x = load(args)
+    B = alg_bytes(A, "f64")
+    vals = np.ascontiguousarray(A.vals, np.float64)
+    y = np.empty(A.nrow)
+    O.spmv_omp_f64(A.row_ptr, A.col, vals, x, y)
+    per_step = []
+    threads = 1
+    # each step: one SpMV over the full matrix on all host cores; the run
+    # stops after ~cpu_seconds even when more steps were requested
+    for _ in range(max(args.warmup, 3)):
+        O.spmv_omp_f64(A.row_ptr, A.col, vals, x, y)
+    t_stop = time.perf_counter() + max(args.cpu_seconds, 5.0) * 3
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, threads = O.spmv_omp_f64(A.row_ptr, A.col, vals, x, y)
+        per_step.append(time.perf_counter() - t0)
+        if time.perf_counter() > t_stop:
+            break
+    sec = statistics.median(per_step)
+    value = B / sec / 1e9
+    out = {
+        "metric": METRIC,
+        "impl": "reference",
+        "value": round(value, 3),
+        "unit": "GB/s",
+        "n_gpus": ws,
+        "steps": len(per_step),
+        "warmup": max(args.warmup, 3),
+        "ms_per_step": round(sec * 1e3, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded generator merbit_b200/synth.py)",
+        "config": {"workload": args.workload, "nrow": A.nrow, "ncol": A.ncol, "nnz": A.nnz,
+                   "values": "f64", "k": 1},
+        "cpu_baseline": {
+            "value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"full {args.workload} matrix per step, median of {len(per_step)} steps; "
+                      "the reference has no CPU SpMV, this is the merge-path OpenMP "
+                      "restatement (oracle/merbit_oracle.c)",
+        },
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    # the reference's own GPU kernel (merbit_kernel<double,256,14>, built from
+    # the reference sources) on the same matrix, for comparison
+    R = O.ref()
+    if R is not None and torch.cuda.is_available():
+        dev = torch.device("cuda", local)
+        rp = torch.from_numpy(A.row_ptr).to(dev)
+        col = torch.from_numpy(A.col).to(dev)
+        v = torch.from_numpy(vals).to(dev)
+        xd = torch.from_numpy(x).to(dev)
+        yd = torch.zeros(A.nrow, dtype=torch.float64, device=dev)
+        zd = torch.zeros(A.nrow, dtype=torch.float64, device=dev)
+        lane_num = (A.nrow + A.nnz + 13) // 14
+        tile_num = (lane_num + 31) // 32
+        tx = torch.zeros(tile_num + 1, dtype=torch.int32, device=dev)
+        ty = torch.zeros(tile_num + 1, dtype=torch.int32, device=dev)
+        desc = torch.zeros(max(lane_num, 1), dtype=torch.int32, device=dev)
+        t0 = time.perf_counter()
+        rc = R.ref_tile_build(14, rp.data_ptr(), A.nrow, A.nnz, tx.data_ptr(), ty.data_ptr(),
+                              desc.data_ptr())
+        t_plan = time.perf_counter() - t0
+        if rc == 0:
+            s = torch.cuda.current_stream(dev).cuda_stream
+            R.ref_merbit_time(0, col.data_ptr(), v.data_ptr(), A.nrow, A.nnz, tx.data_ptr(),
+                              ty.data_ptr(), desc.data_ptr(), xd.data_ptr(), yd.data_ptr(),
+                              zd.data_ptr(), 10, s)
+            ms = R.ref_merbit_time(0, col.data_ptr(), v.data_ptr(), A.nrow, A.nnz,
+                                   tx.data_ptr(), ty.data_ptr(), desc.data_ptr(), xd.data_ptr(),
+                                   yd.data_ptr(), zd.data_ptr(), 400, s)
+            out["ref_gpu_kernel"] = {
+                "kernel": "merbit_kernel<double,256,14> (reference source, sm_100a build)",
+                "value": round(B / (ms * 1e-3) / 1e9, 2), "unit": "GB/s",
+                "ms_per_spmv": round(float(ms), 5), "reps": 400,
+                "plan_build_s_host_wall": round(t_plan, 4),
+            }
+    print(json.dumps(out), flush=True)
+    if ws > 1:
+        barrier(ws)
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,138 @@
+/*
+ * merbit_b200: merge-path tiled CSR SpMV / SpMM for NVIDIA B200 (sm_100a).
+ *
+ * C ABI (plain pointers, sizes, int status).  All matrix, vector and
+ * scratch pointers are DEVICE pointers on the current CUDA device unless
+ * stated otherwise; `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).  Every entry point returns a merbit_status.
+ *
+ * Reference interfaces replaced (paths relative to the MERBIT project root):
+ *
+ *   merbit_merge_coords   merge_search<SIGMA>            include/utils.cuh:5-29
+ *   merbit_tile_dims      TILE<BLOCK,SIGMA> sizes         include/tile.cuh:114-115
+ *   merbit_tile_build     TILE ctor + Tile_Kernel         include/tile.cuh:4-25,28-122
+ *   merbit_plan_create    offset build + TILE in          include/tile.cuh:571-593
+ *                         Fun_Merbit (sort is the caller's; see merbit_coo_to_csr)
+ *   merbit_spmv           merbit_kernel launch            include/tile.cuh:476-561,596-603
+ *                         (y = alpha*A*x; beta extends it)
+ *   merbit_spmm           (k right-hand sides; no reference counterpart, same kernel family)
+ *   merbit_spmm_t         adjoint dX = A^T G              (no reference counterpart)
+ *   merbit_dval           adjoint dval = G[row].X[col]    (no reference counterpart)
+ *   merbit_coo_to_csr     GRAPH::sort(false) +            src/class.cu:143-177,
+ *                         cusparseXcoo2csr                 include/tile.cuh:571-574
+ *   merbit_pagerank_step  PARAMETER damping scaffold      include/class.cuh:119-146
+ *
+ * Threading: a plan may be used from any host thread, but launches that use
+ * the same plan must be ordered on the device (one stream, or ordered by
+ * events): each plan owns device scratch (carry slots, a launch counter)
+ * that every launch reuses.  The reference is single-stream as well
+ * (include/tile.cuh:596-603).
+ */
+#ifndef MERBIT_H
+#define MERBIT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum merbit_status {
+    MERBIT_OK = 0,
+    MERBIT_ERR_INVALID = 1,     /* bad argument: null pointer, negative size, bad dtype/k/ld */
+    MERBIT_ERR_MATRIX = 2,      /* row_ptr[0]!=0, row_ptr[nrow]!=nnz, decreasing row_ptr,
+                                   or a column index outside [0,ncol) */
+    MERBIT_ERR_OVERFLOW = 3,    /* nrow+nnz beyond the int32 merge-path range */
+    MERBIT_ERR_CUDA = 4,        /* a CUDA runtime call failed: merbit_last_cuda_error() */
+    MERBIT_ERR_TIMEOUT = 5,     /* a device-side carry wait ran out (bounded spin); the
+                                   launch's output is invalid; reported by merbit_plan_check */
+    MERBIT_ERR_UNSUPPORTED = 6  /* valid request this build does not implement */
+} merbit_status;
+
+typedef enum merbit_dtype {
+    MERBIT_F64 = 0,  /* values f64; x, y f64; f64 accumulation (the plain form) */
+    MERBIT_F32 = 1,  /* values f32; x, y f32; f32 two-sum accumulation, f64 carries */
+    MERBIT_BF16 = 2  /* values bf16; x, y f32; f32 two-sum accumulation, f64 carries */
+} merbit_dtype;
+
+/* merbit_plan_create flags */
+#define MERBIT_PLAN_SKIP_VALIDATE 0x1u /* trust row_ptr/col_idx (skips one pass + a sync) */
+#define MERBIT_PLAN_NO_TUNE 0x2u       /* never time candidate configurations */
+
+typedef struct merbit_plan_s* merbit_plan;
+
+typedef struct merbit_plan_info {
+    int32_t nrow, ncol, nnz;
+    int32_t dtype;
+    int32_t block;           /* threads per CTA of the SpMV kernel in use */
+    int32_t items_per_thread;/* merge items per thread */
+    int32_t tile_items;      /* merge items (row ends + nonzeros) per tile */
+    int32_t num_tiles;
+    int32_t vectorized;      /* 1 when 128-bit loads of col_idx/vals are used */
+    int64_t metadata_bytes;  /* partition + carry scratch held by the plan */
+    double algorithmic_bytes;/* compulsory bytes of one SpMV, y = A x */
+} merbit_plan_info;
+
+/* ---------------- reference-format partition (parity surface) ---------------- */
+
+/* Merge-path coordinates at diagonals i*stride (clamped to nrow+nnz), i in
+ * [0,count): d_coord_x[i] = nonzeros consumed, d_coord_y[i] = rows consumed.
+ * Bit-identical to merge_search (include/utils.cuh:5-29), tie rule included. */
+int merbit_merge_coords(const int32_t* d_row_ptr, int32_t nrow, int32_t nnz, int64_t stride,
+                        int64_t count, int32_t* d_coord_x, int32_t* d_coord_y, void* stream);
+
+/* TILE<BLOCK,SIGMA> sizes: lane_num = ceil((nrow+nnz)/sigma), tile_num =
+ * ceil(lane_num/32) (include/tile.cuh:114-115). */
+int merbit_tile_dims(int32_t nrow, int32_t nnz, int32_t sigma, int32_t* tile_num,
+                     int32_t* lane_num);
+
+/* The reference's Merbit plan, bit for bit (include/tile.cuh:28-104):
+ * d_tile_x[tile_num+1], d_tile_y[tile_num+1] (MSB = "fast" tile with no row
+ * end), d_lane_desc[lane_num] of 4-byte descriptors when sigma < 15 and
+ * 8-byte ones otherwise.  1 <= sigma <= 42. */
+int merbit_tile_build(const int32_t* d_row_ptr, int32_t nrow, int32_t nnz, int32_t sigma,
+                      uint32_t* d_tile_x, uint32_t* d_tile_y, void* d_lane_desc, void* stream);
+
+/* ---------------- plans: y = alpha*A*x + beta*y ---------------- */
+
+/* Builds the partition and carry scratch for one CSR matrix (square or not).
+ * The plan keeps the caller's device pointers (it copies nothing): they must
+ * stay valid and unchanged in structure while the plan lives.  Validates the
+ * structure unless MERBIT_PLAN_SKIP_VALIDATE.  Synchronizes `stream`. */
+int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nnz,
+                       const int32_t* d_row_ptr, const int32_t* d_col_idx, const void* d_vals,
+                       merbit_dtype dtype, uint32_t flags, void* stream);
+int merbit_plan_destroy(merbit_plan plan);
+int merbit_plan_get_info(merbit_plan plan, merbit_plan_info* info);
+
+/* Replace the value array (same structure, same dtype). */
+int merbit_plan_set_values(merbit_plan plan, const void* d_vals);
+
+/* Selects the SpMV kernel configuration by timing the candidates on this
+ * matrix (`x`,`y` are scratch vectors of the plan's dtype, contents
+ * overwritten).  The choice is cached per matrix signature for the process.
+ * Not capturable (it synchronizes). */
+int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream);
+
+/* y[nrow] = alpha*A*x[ncol] + beta*y.  beta == 0 never reads y. */
+int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
+                void* stream);
+
+/* Reads and clears the plan's device-side status (MERBIT_ERR_TIMEOUT if a
+ * carry wait ran out in any launch since the last check).  Synchronizes. */
+int merbit_plan_check(merbit_plan plan, void* stream);
+
+/* ---------------- errors ---------------- */
+
+const char* merbit_status_string(int status);
+/* Last cudaError_t seen by this thread inside the library (0 if none). */
+int merbit_last_cuda_error(void);
+/* Human-readable detail of this thread's last failure ("" if none). */
+const char* merbit_last_error_detail(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MERBIT_H */

@@ -1,0 +1,257 @@
+"""merbit_b200: merge-path tiled CSR SpMV/SpMM for NVIDIA B200 (sm_100a).
+
+Python host side of the C ABI declared in ``include/merbit.h``.  PyTorch
+supplies device memory and streams; every operation runs in the hand-written
+CUDA kernels of ``libmerbit_b200.so`` (built in-tree by
+``python -m merbit_b200._build``).  There is no CPU fallback: importing the
+operations without the library raises.
+
+Reference interfaces mirrored (paths relative to the MERBIT project root):
+
+* ``merge_coords``  -> ``merge_search<SIGMA>``   include/utils.cuh:5-29
+* ``tile_build``    -> ``TILE<BLOCK,SIGMA>``     include/tile.cuh:4-122
+* ``Plan.spmv``     -> ``merbit_kernel`` via ``Fun_Merbit``
+                       include/tile.cuh:476-615
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import torch
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmerbit_b200.so")
+
+F64, F32, BF16 = 0, 1, 2
+PLAN_SKIP_VALIDATE = 0x1
+PLAN_NO_TUNE = 0x2
+
+_DT_OF = {torch.float64: F64, torch.float32: F32, torch.bfloat16: BF16}
+_XY_OF = {F64: torch.float64, F32: torch.float32, BF16: torch.float32}
+
+STATUS = {
+    0: "MERBIT_OK",
+    1: "MERBIT_ERR_INVALID",
+    2: "MERBIT_ERR_MATRIX",
+    3: "MERBIT_ERR_OVERFLOW",
+    4: "MERBIT_ERR_CUDA",
+    5: "MERBIT_ERR_TIMEOUT",
+    6: "MERBIT_ERR_UNSUPPORTED",
+}
+
+
+class MerbitError(RuntimeError):
+    def __init__(self, status: int, detail: str):
+        self.status = status
+        self.detail = detail
+        super().__init__(f"{STATUS.get(status, status)}: {detail}")
+
+
+class _PlanInfo(C.Structure):
+    _fields_ = [
+        ("nrow", C.c_int32), ("ncol", C.c_int32), ("nnz", C.c_int32), ("dtype", C.c_int32),
+        ("block", C.c_int32), ("items_per_thread", C.c_int32), ("tile_items", C.c_int32),
+        ("num_tiles", C.c_int32), ("vectorized", C.c_int32),
+        ("metadata_bytes", C.c_int64), ("algorithmic_bytes", C.c_double),
+    ]
+
+
+_P = C.c_void_p
+# name -> (restype, argtypes); the complete exported surface of include/merbit.h
+SIGNATURES = {
+    "merbit_merge_coords": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int64, C.c_int64, _P, _P, _P]),
+    "merbit_tile_dims": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P]),
+    "merbit_tile_build": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P]),
+    "merbit_plan_create": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int,
+                                     C.c_uint32, _P]),
+    "merbit_plan_destroy": (C.c_int, [_P]),
+    "merbit_plan_get_info": (C.c_int, [_P, _P]),
+    "merbit_plan_set_values": (C.c_int, [_P, _P]),
+    "merbit_plan_tune": (C.c_int, [_P, _P, _P, _P]),
+    "merbit_spmv": (C.c_int, [_P, C.c_double, _P, C.c_double, _P, _P]),
+    "merbit_plan_check": (C.c_int, [_P, _P]),
+    "merbit_status_string": (C.c_char_p, [C.c_int]),
+    "merbit_last_cuda_error": (C.c_int, []),
+    "merbit_last_error_detail": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The native library, with argument types set.  Raises if it is not
+    built: there is no fallback path."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing; build it with `python -m merbit_b200._build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        detail = lib().merbit_last_error_detail().decode(errors="replace")
+        raise MerbitError(status, detail)
+
+
+def _stream_ptr(stream) -> _P:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return _P(stream.cuda_stream)
+
+
+def _dptr(t: torch.Tensor | None) -> _P:
+    return _P(t.data_ptr()) if t is not None else _P(0)
+
+
+def _need_cuda(t: torch.Tensor, name: str, dtype=None) -> None:
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def merge_coords(row_ptr: torch.Tensor, nnz: int, stride: int, count: int, stream=None):
+    """Merge-path coordinates at diagonals i*stride (include/utils.cuh:5-29).
+    Returns int32 tensors (coord_x, coord_y)."""
+    _need_cuda(row_ptr, "row_ptr", torch.int32)
+    cx = torch.empty(count, dtype=torch.int32, device=row_ptr.device)
+    cy = torch.empty(count, dtype=torch.int32, device=row_ptr.device)
+    _check(lib().merbit_merge_coords(_dptr(row_ptr), row_ptr.numel() - 1, nnz, stride, count,
+                                     _dptr(cx), _dptr(cy), _stream_ptr(stream)))
+    return cx, cy
+
+
+def tile_dims(nrow: int, nnz: int, sigma: int) -> tuple[int, int]:
+    t, l = C.c_int32(), C.c_int32()
+    _check(lib().merbit_tile_dims(nrow, nnz, sigma, C.byref(t), C.byref(l)))
+    return t.value, l.value
+
+
+def tile_build(row_ptr: torch.Tensor, nnz: int, sigma: int = 14, stream=None):
+    """The reference Merbit plan (TILE<BLOCK,SIGMA>, include/tile.cuh:4-122):
+    (tile_x u32[T+1], tile_y u32[T+1], lane_desc u32|u64[lane_num]) as int32 /
+    int64 tensors holding the same bits."""
+    _need_cuda(row_ptr, "row_ptr", torch.int32)
+    nrow = row_ptr.numel() - 1
+    T, Ln = tile_dims(nrow, nnz, sigma)
+    dev = row_ptr.device
+    tx = torch.empty(T + 1, dtype=torch.int32, device=dev)
+    ty = torch.empty(T + 1, dtype=torch.int32, device=dev)
+    desc = torch.empty(max(Ln, 1), dtype=torch.int32 if sigma < 15 else torch.int64, device=dev)
+    _check(lib().merbit_tile_build(_dptr(row_ptr), nrow, nnz, sigma, _dptr(tx), _dptr(ty),
+                                   _dptr(desc), _stream_ptr(stream)))
+    return tx, ty, desc[:Ln]
+
+
+@dataclass
+class PlanInfo:
+    nrow: int
+    ncol: int
+    nnz: int
+    dtype: int
+    block: int
+    items_per_thread: int
+    tile_items: int
+    num_tiles: int
+    vectorized: bool
+    metadata_bytes: int
+    algorithmic_bytes: float
+
+
+class Plan:
+    """One CSR matrix prepared for repeated products (merbit_plan_create).
+
+    row_ptr / col_idx: int32 CUDA tensors; vals: float64, float32 or bfloat16
+    CUDA tensor.  x and y are float64 for float64 values and float32 otherwise.
+    The plan references (does not copy) the tensors and keeps them alive.
+    """
+
+    def __init__(self, row_ptr: torch.Tensor, col_idx: torch.Tensor, vals: torch.Tensor,
+                 ncol: int | None = None, validate: bool = True, stream=None):
+        _need_cuda(row_ptr, "row_ptr", torch.int32)
+        _need_cuda(col_idx, "col_idx", torch.int32)
+        _need_cuda(vals, "vals")
+        if vals.dtype not in _DT_OF:
+            raise TypeError(f"unsupported value dtype {vals.dtype}")
+        self.dtype = _DT_OF[vals.dtype]
+        self.xy_dtype = _XY_OF[self.dtype]
+        self.nrow = row_ptr.numel() - 1
+        self.nnz = col_idx.numel()
+        self.ncol = self.nrow if ncol is None else int(ncol)
+        self.device = row_ptr.device
+        self._keep = [row_ptr, col_idx, vals]
+        self.row_ptr, self.col_idx, self.vals = row_ptr, col_idx, vals
+        self._h = _P()
+        flags = 0 if validate else PLAN_SKIP_VALIDATE
+        with torch.cuda.device(self.device):
+            _check(lib().merbit_plan_create(C.byref(self._h), self.nrow, self.ncol, self.nnz,
+                                            _dptr(row_ptr), _dptr(col_idx), _dptr(vals),
+                                            self.dtype, flags, _stream_ptr(stream)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().merbit_plan_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> PlanInfo:
+        i = _PlanInfo()
+        _check(lib().merbit_plan_get_info(self._h, C.byref(i)))
+        return PlanInfo(i.nrow, i.ncol, i.nnz, i.dtype, i.block, i.items_per_thread,
+                        i.tile_items, i.num_tiles, bool(i.vectorized), i.metadata_bytes,
+                        i.algorithmic_bytes)
+
+    def set_values(self, vals: torch.Tensor) -> None:
+        _need_cuda(vals, "vals", self.vals.dtype)
+        if vals.numel() != self.nnz:
+            raise ValueError("vals has the wrong length")
+        _check(lib().merbit_plan_set_values(self._h, _dptr(vals)))
+        self.vals = vals
+        self._keep[2] = vals
+
+    def _vec(self, t: torch.Tensor, n: int, name: str) -> None:
+        _need_cuda(t, name, self.xy_dtype)
+        if t.numel() != n:
+            raise ValueError(f"{name} must have {n} elements, got {t.numel()}")
+
+    def spmv(self, x: torch.Tensor, y: torch.Tensor | None = None, alpha: float = 1.0,
+             beta: float = 0.0, stream=None) -> torch.Tensor:
+        """y = alpha*A*x + beta*y (beta == 0 never reads y)."""
+        self._vec(x, self.ncol, "x")
+        if y is None:
+            y = torch.empty(self.nrow, dtype=self.xy_dtype, device=self.device)
+        else:
+            self._vec(y, self.nrow, "y")
+        _check(lib().merbit_spmv(self._h, float(alpha), _dptr(x), float(beta), _dptr(y),
+                                 _stream_ptr(stream)))
+        return y
+
+    def tune(self, x: torch.Tensor | None = None, stream=None) -> PlanInfo:
+        """Time every kernel configuration on this matrix and keep the fastest
+        (cached per matrix signature for the process)."""
+        if x is None:
+            x = torch.ones(self.ncol, dtype=self.xy_dtype, device=self.device)
+        y = torch.empty(self.nrow, dtype=self.xy_dtype, device=self.device)
+        _check(lib().merbit_plan_tune(self._h, _dptr(x), _dptr(y), _stream_ptr(stream)))
+        return self.info()
+
+    def check(self, stream=None) -> None:
+        """Raise MerbitError if a device-side wait of any launch ran out."""
+        _check(lib().merbit_plan_check(self._h, _stream_ptr(stream)))

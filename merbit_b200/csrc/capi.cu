@@ -1,0 +1,317 @@
+// C ABI: plan lifetime, SpMV dispatch, tuning, error reporting.
+//
+// The plan plays the part of the reference's per-call setup in Fun_Merbit
+// (include/tile.cuh:563-615: offset build, TILE construction, y/z buffers),
+// done once and reused: the partition for the chosen tile size and the
+// carry slots stay resident in HBM across launches.
+#include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "merbit_internal.cuh"
+
+namespace merbit {
+
+namespace {
+thread_local std::string g_detail;
+thread_local int g_last_cuda = 0;
+}  // namespace
+
+void set_error_detail(const std::string& s) { g_detail = s; }
+
+int fail(int status, const std::string& detail) {
+    g_detail = detail;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    g_last_cuda = (int)e;
+    g_detail = std::string(where) + ": " + cudaGetErrorString(e);
+    return MERBIT_ERR_CUDA;
+}
+
+int validate_csr(const int32_t* row_ptr, const int32_t* col, int nrow, int ncol, int nnz,
+                 cudaStream_t s);
+
+namespace {
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Ensures the plan holds a partition for `tile_items` and enough carry
+// slots; returns it in *out.
+int plan_partition(merbit_plan_s* p, int tile_items, const Partition** out, cudaStream_t s) {
+    for (auto& q : p->parts)
+        if (q.tile_items == tile_items) {
+            *out = &q;
+            return MERBIT_OK;
+        }
+    Partition q;
+    int st = build_partition(p->row_ptr, p->nrow, p->nnz, tile_items, &q, s);
+    if (st != MERBIT_OK) return st;
+    if (q.num_tiles > p->slots) {
+        // grow the carry slots; flags start at 0 which never equals a live
+        // epoch (epochs start at 1 and only increase)
+        MERBIT_CUDA(cudaStreamSynchronize(s));
+        cudaFree(p->agg);
+        cudaFree(p->flag);
+        p->agg = nullptr;
+        p->flag = nullptr;
+        MERBIT_CUDA(cudaMalloc(&p->agg, sizeof(double) * (size_t)q.num_tiles));
+        MERBIT_CUDA(cudaMalloc(&p->flag, sizeof(unsigned) * (size_t)q.num_tiles));
+        MERBIT_CUDA(cudaMemsetAsync(p->flag, 0, sizeof(unsigned) * (size_t)q.num_tiles, s));
+        // restart epochs so no stale flag can match
+        LaunchState init = {};
+        init.epoch = 1u;
+        MERBIT_CUDA(cudaMemcpyAsync(p->state, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+        MERBIT_CUDA(cudaStreamSynchronize(s));
+        p->slots = q.num_tiles;
+    }
+    p->parts.push_back(q);
+    *out = &p->parts.back();
+    return MERBIT_OK;
+}
+
+int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta, void* y,
+             cudaStream_t s) {
+    const SpmvConfig c = spmv_config(p->dtype, cfg);
+    const Partition* part = nullptr;
+    int st = plan_partition(p, c.block * c.ipt, &part, s);
+    if (st != MERBIT_OK) return st;
+    SpmvLaunch a;
+    a.row_ptr = p->row_ptr;
+    a.col = p->col;
+    a.vals = p->vals;
+    a.x = x;
+    a.y = y;
+    a.coords = part->coords;
+    a.agg = p->agg;
+    a.flag = p->flag;
+    a.state = p->state;
+    a.num_tiles = part->num_tiles;
+    a.alpha = alpha;
+    a.beta = beta;
+    return spmv_launch(p->dtype, cfg, p->vec, a, s);
+}
+
+// Tuning cache: matrix signature -> config index.
+struct Sig {
+    int dtype, vec, nrow_bucket, nnz_bucket, density_bucket;
+    bool operator<(const Sig& o) const {
+        return std::tie(dtype, vec, nrow_bucket, nnz_bucket, density_bucket) <
+               std::tie(o.dtype, o.vec, o.nrow_bucket, o.nnz_bucket, o.density_bucket);
+    }
+};
+std::mutex g_tune_mu;
+std::map<Sig, int> g_tune;
+
+int log2_bucket(double v) {
+    int b = 0;
+    while (v >= 2.0 && b < 62) {
+        v *= 0.5;
+        ++b;
+    }
+    return b;
+}
+
+Sig signature(const merbit_plan_s* p) {
+    Sig s;
+    s.dtype = p->dtype;
+    s.vec = p->vec;
+    s.nrow_bucket = log2_bucket((double)p->nrow);
+    s.nnz_bucket = log2_bucket((double)p->nnz);
+    s.density_bucket = log2_bucket(4.0 * (double)p->nnz / (double)(p->nrow > 0 ? p->nrow : 1));
+    return s;
+}
+
+}  // namespace
+}  // namespace merbit
+
+using namespace merbit;
+
+extern "C" {
+
+const char* merbit_status_string(int status) {
+    switch (status) {
+    case MERBIT_OK: return "MERBIT_OK";
+    case MERBIT_ERR_INVALID: return "MERBIT_ERR_INVALID: invalid argument";
+    case MERBIT_ERR_MATRIX: return "MERBIT_ERR_MATRIX: malformed CSR structure";
+    case MERBIT_ERR_OVERFLOW: return "MERBIT_ERR_OVERFLOW: nrow+nnz exceeds the int32 range";
+    case MERBIT_ERR_CUDA: return "MERBIT_ERR_CUDA: CUDA runtime error";
+    case MERBIT_ERR_TIMEOUT: return "MERBIT_ERR_TIMEOUT: device-side carry wait ran out";
+    case MERBIT_ERR_UNSUPPORTED: return "MERBIT_ERR_UNSUPPORTED: not implemented";
+    default: return "MERBIT: unknown status";
+    }
+}
+
+int merbit_last_cuda_error(void) { return g_last_cuda; }
+
+const char* merbit_last_error_detail(void) { return g_detail.c_str(); }
+
+int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nnz,
+                       const int32_t* d_row_ptr, const int32_t* d_col_idx, const void* d_vals,
+                       merbit_dtype dtype, uint32_t flags, void* stream) {
+    if (!plan) return fail(MERBIT_ERR_INVALID, "plan_create: plan is null");
+    *plan = nullptr;
+    if (nrow < 0 || ncol < 0 || nnz < 0) return fail(MERBIT_ERR_INVALID, "plan_create: negative size");
+    if (dtype != MERBIT_F64 && dtype != MERBIT_F32 && dtype != MERBIT_BF16)
+        return fail(MERBIT_ERR_INVALID, "plan_create: unknown dtype");
+    if (!d_row_ptr) return fail(MERBIT_ERR_INVALID, "plan_create: row_ptr is null");
+    if (nnz > 0 && (!d_col_idx || !d_vals))
+        return fail(MERBIT_ERR_INVALID, "plan_create: col_idx/vals null with nnz > 0");
+    if (nnz > 0 && ncol == 0) return fail(MERBIT_ERR_MATRIX, "plan_create: nnz > 0 with ncol == 0");
+    if ((long long)nrow + nnz > (long long)INT_MAX - 64)
+        return fail(MERBIT_ERR_OVERFLOW, "plan_create: nrow+nnz exceeds the int32 merge-path range");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!(flags & MERBIT_PLAN_SKIP_VALIDATE)) {
+        int st = validate_csr(d_row_ptr, d_col_idx, nrow, ncol, nnz, s);
+        if (st != MERBIT_OK) return st;
+    }
+    auto* p = new merbit_plan_s();
+    p->nrow = nrow;
+    p->ncol = ncol;
+    p->nnz = nnz;
+    p->dtype = dtype;
+    p->row_ptr = d_row_ptr;
+    p->col = d_col_idx;
+    p->vals = d_vals;
+    p->vec = aligned16(d_col_idx) && aligned16(d_vals);
+    cudaGetDevice(&p->device);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(signature(p));
+        p->cfg = it != g_tune.end() ? it->second : spmv_default_config(dtype, nrow, nnz);
+    }
+    cudaError_t e = cudaMalloc(&p->state, sizeof(LaunchState));
+    if (e != cudaSuccess) {
+        delete p;
+        return cuda_fail(e, "plan_create: cudaMalloc(state)");
+    }
+    LaunchState init = {};
+    init.epoch = 1u;
+    e = cudaMemcpyAsync(p->state, &init, sizeof(init), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        merbit_plan_destroy(p);
+        return cuda_fail(e, "plan_create: init state");
+    }
+    const SpmvConfig c = spmv_config(dtype, p->cfg);
+    const Partition* part = nullptr;
+    int st = plan_partition(p, c.block * c.ipt, &part, s);
+    if (st == MERBIT_OK) {
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(e, "plan_create: sync");
+    }
+    if (st != MERBIT_OK) {
+        merbit_plan_destroy(p);
+        return st;
+    }
+    *plan = p;
+    return MERBIT_OK;
+}
+
+int merbit_plan_destroy(merbit_plan plan) {
+    if (!plan) return MERBIT_OK;
+    for (auto& q : plan->parts) cudaFree(q.coords);
+    cudaFree(plan->agg);
+    cudaFree(plan->flag);
+    cudaFree(plan->state);
+    delete plan;
+    return MERBIT_OK;
+}
+
+int merbit_plan_get_info(merbit_plan plan, merbit_plan_info* info) {
+    if (!plan || !info) return fail(MERBIT_ERR_INVALID, "plan_get_info: null pointer");
+    const SpmvConfig c = spmv_config(plan->dtype, plan->cfg);
+    info->nrow = plan->nrow;
+    info->ncol = plan->ncol;
+    info->nnz = plan->nnz;
+    info->dtype = plan->dtype;
+    info->block = c.block;
+    info->items_per_thread = c.ipt;
+    info->tile_items = c.block * c.ipt;
+    info->num_tiles = 0;
+    int64_t meta = sizeof(LaunchState) + (int64_t)plan->slots * (sizeof(double) + sizeof(unsigned));
+    for (auto& q : plan->parts) {
+        if (q.tile_items == info->tile_items) info->num_tiles = q.num_tiles;
+        meta += (int64_t)(q.num_tiles + 1) * (int64_t)sizeof(int2);
+    }
+    info->vectorized = plan->vec ? 1 : 0;
+    info->metadata_bytes = meta;
+    info->algorithmic_bytes = 4.0 * (plan->nrow + 1.0) +
+                              (double)plan->nnz * (4.0 + (double)dtype_size(plan->dtype)) +
+                              (double)xy_size(plan->dtype) * ((double)plan->ncol + plan->nrow);
+    return MERBIT_OK;
+}
+
+int merbit_plan_set_values(merbit_plan plan, const void* d_vals) {
+    if (!plan) return fail(MERBIT_ERR_INVALID, "plan_set_values: plan is null");
+    if (plan->nnz > 0 && !d_vals) return fail(MERBIT_ERR_INVALID, "plan_set_values: vals is null");
+    plan->vals = d_vals;
+    plan->vec = aligned16(plan->col) && aligned16(d_vals);
+    return MERBIT_OK;
+}
+
+int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
+                void* stream) {
+    if (!plan) return fail(MERBIT_ERR_INVALID, "spmv: plan is null");
+    if (plan->nrow == 0) return MERBIT_OK;
+    if (!d_y || (plan->ncol > 0 && !d_x)) return fail(MERBIT_ERR_INVALID, "spmv: x/y is null");
+    return run_spmv(plan, plan->cfg, alpha, d_x, beta, d_y, (cudaStream_t)stream);
+}
+
+int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream) {
+    if (!plan) return fail(MERBIT_ERR_INVALID, "plan_tune: plan is null");
+    if (plan->nrow == 0) return MERBIT_OK;
+    if (!d_y || (plan->ncol > 0 && !d_x)) return fail(MERBIT_ERR_INVALID, "plan_tune: x/y is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    MERBIT_CUDA(cudaEventCreate(&e0));
+    MERBIT_CUDA(cudaEventCreate(&e1));
+    const int n = spmv_num_configs(plan->dtype);
+    int best = plan->cfg;
+    float best_ms = 1e30f;
+    int st = MERBIT_OK;
+    for (int c = 0; c < n && st == MERBIT_OK; ++c) {
+        for (int w = 0; w < 2 && st == MERBIT_OK; ++w) st = run_spmv(plan, c, 1.0, d_x, 0.0, d_y, s);
+        if (st != MERBIT_OK) break;
+        const int reps = 5;
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps && st == MERBIT_OK; ++r) st = run_spmv(plan, c, 1.0, d_x, 0.0, d_y, s);
+        cudaEventRecord(e1, s);
+        cudaError_t ce = cudaEventSynchronize(e1);
+        if (ce != cudaSuccess) {
+            st = cuda_fail(ce, "plan_tune");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != MERBIT_OK) return st;
+    plan->cfg = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[signature(plan)] = best;
+    return MERBIT_OK;
+}
+
+int merbit_plan_check(merbit_plan plan, void* stream) {
+    if (!plan) return fail(MERBIT_ERR_INVALID, "plan_check: plan is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    int err = 0;
+    MERBIT_CUDA(cudaMemcpyAsync(&err, &plan->state->error, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MERBIT_CUDA(cudaStreamSynchronize(s));
+    if (err != 0) {
+        const int zero = 0;
+        MERBIT_CUDA(cudaMemcpyAsync(&plan->state->error, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+        MERBIT_CUDA(cudaStreamSynchronize(s));
+        return fail(err, "a device-side carry wait ran out");
+    }
+    return MERBIT_OK;
+}
+
+}  // extern "C"

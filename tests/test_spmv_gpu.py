@@ -1,0 +1,206 @@
+"""SpMV parity on the GPU, through the C ABI.
+
+Tolerances (component-wise, e_i = |y_i - y*_i| / sum_j |a_ij x_j| against
+the extended-precision oracle computed on the stored values):
+  * f64 (plain form):            1e-13
+  * f32 / bf16 (precision form): 1e-6   (the target north_star states)
+and against the reference merbit_kernel (oracle/_ref, its own float atomics):
+  * f64: 1e-12,  f32: 1e-5 (the reference accumulates in plain float)
+"""
+import numpy as np
+import pytest
+import torch
+
+import merbit_b200 as mb
+from merbit_b200 import synth
+from oracle import oracle as O
+from tests.helpers import csr_from_lengths, edge_cases, stored_values, to_cuda
+
+CASES = edge_cases()
+TOL = {"f64": 1e-13, "f32": 1e-6, "bf16": 1e-6}
+XT = {"f64": torch.float64, "f32": torch.float32, "bf16": torch.float32}
+
+
+def _x(A, dtype, seed=7):
+    x = synth.uniform(seed, A.ncol)
+    return x.astype(np.float64 if dtype == "f64" else np.float32)
+
+
+def _run(A, dtype, x, alpha=1.0, beta=0.0, y0=None, tune=False):
+    rp, col, v = to_cuda(A, dtype)
+    plan = mb.Plan(rp, col, v, ncol=A.ncol)
+    if tune:
+        plan.tune()
+    xd = torch.from_numpy(x).cuda()
+    y = None if y0 is None else torch.from_numpy(y0).cuda()
+    y = plan.spmv(xd, y, alpha=alpha, beta=beta)
+    torch.cuda.synchronize()
+    plan.check()
+    return plan, y.cpu().numpy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
+@pytest.mark.parametrize("name,A", CASES, ids=[c[0] for c in CASES])
+def test_spmv_vs_oracle(name, A, dtype):
+    x = _x(A, dtype)
+    _, y = _run(A, dtype, x)
+    yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+    emax, emed = O.rel_error(y, yo, ya)
+    assert emax <= TOL[dtype], (emax, emed)
+    # rows with no nonzeros are exactly zero
+    empty = np.diff(A.row_ptr) == 0
+    assert np.all(y[empty] == 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
+def test_spmv_every_config(dtype):
+    """Every tile configuration the tuner can pick gives the oracle's answer."""
+    A = synth.workload("zipf_small")
+    x = _x(A, dtype)
+    yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+    rp, col, v = to_cuda(A, dtype)
+    plan = mb.Plan(rp, col, v)
+    plan.tune(torch.from_numpy(x).cuda())
+    y = plan.spmv(torch.from_numpy(x).cuda())
+    assert O.rel_error(y.cpu().numpy(), yo, ya)[0] <= TOL[dtype]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_alpha_beta(dtype):
+    A = synth.workload("zipf_small")
+    x = _x(A, dtype)
+    y0 = synth.uniform(11, A.nrow).astype(x.dtype)
+    _, y = _run(A, dtype, x, alpha=-2.5, beta=0.75, y0=y0)
+    yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x, alpha=-2.5)
+    ref = yo + 0.75 * y0.astype(np.float64)
+    err = np.abs(y - ref) / np.maximum(ya + 0.75 * np.abs(y0), 1e-300)
+    assert err.max() <= TOL[dtype] * 4
+
+
+@pytest.mark.gpu
+def test_beta_zero_ignores_nan_in_y():
+    A = synth.workload("laplace2d_small")
+    x = _x(A, "f64")
+    y0 = np.full(A.nrow, np.nan)
+    _, y = _run(A, "f64", x, beta=0.0, y0=y0)
+    assert np.isfinite(y).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_deterministic_bitwise(dtype):
+    """No float atomics: repeated launches give identical bits."""
+    A = csr_from_lengths([0, 70_000, 5, 0, 90_000, 1] * 3, ncol=200_000, seed=9)
+    x = _x(A, dtype)
+    rp, col, v = to_cuda(A, dtype)
+    plan = mb.Plan(rp, col, v, ncol=A.ncol)
+    xd = torch.from_numpy(x).cuda()
+    ys = [plan.spmv(xd).clone() for _ in range(20)]
+    for y in ys[1:]:
+        assert torch.equal(y.view(torch.int64 if dtype == "f64" else torch.int32),
+                           ys[0].view(torch.int64 if dtype == "f64" else torch.int32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
+def test_unaligned_pointers_scalar_path(dtype):
+    """Views that start off a 16-byte boundary take the scalar-load kernel."""
+    A = synth.workload("zipf_small")
+    rp, col, v = to_cuda(A, dtype)
+    col2 = torch.empty(col.numel() + 1, dtype=col.dtype, device="cuda")
+    col2[1:] = col
+    v2 = torch.empty(v.numel() + 1, dtype=v.dtype, device="cuda")
+    v2[1:] = v
+    plan = mb.Plan(rp, col2[1:], v2[1:])
+    assert not plan.info().vectorized
+    x = _x(A, dtype)
+    y = plan.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
+    yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+    assert O.rel_error(y, yo, ya)[0] <= TOL[dtype]
+
+
+@pytest.mark.gpu
+def test_rectangular():
+    A = csr_from_lengths(np.arange(300) % 17, ncol=50_000, seed=12)
+    x = _x(A, "f64")
+    _, y = _run(A, "f64", x)
+    yo, ya = O.spmm(A.row_ptr, A.col, A.vals, x)
+    assert O.rel_error(y, yo, ya)[0] <= TOL["f64"]
+
+
+@pytest.mark.gpu
+def test_empty_matrix():
+    rp = torch.zeros(1, dtype=torch.int32, device="cuda")
+    col = torch.zeros(0, dtype=torch.int32, device="cuda")
+    v = torch.zeros(0, dtype=torch.float64, device="cuda")
+    plan = mb.Plan(rp, col, v, ncol=0)
+    y = plan.spmv(torch.zeros(0, dtype=torch.float64, device="cuda"))
+    assert y.numel() == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bad", ["rp0", "rpn", "decreasing", "col_high", "col_neg"])
+def test_malformed_structure_rejected(bad):
+    A = synth.workload("laplace2d_small")
+    rp, col, v = A.row_ptr.copy(), A.col.copy(), A.vals
+    if bad == "rp0":
+        rp[0] = 1
+    elif bad == "rpn":
+        rp[-1] -= 1
+    elif bad == "decreasing":
+        rp[10] = rp[12] + 1
+    elif bad == "col_high":
+        col[100] = A.ncol
+    else:
+        col[5] = -1
+    with pytest.raises(mb.MerbitError) as ei:
+        mb.Plan(torch.from_numpy(rp).cuda(), torch.from_numpy(col).cuda(),
+                torch.from_numpy(v).cuda(), ncol=A.ncol)
+    assert ei.value.status == 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_vs_reference_merbit_kernel(dtype):
+    """Same y as the reference merbit_kernel<V,256,14> run on this GPU."""
+    R = O.ref()
+    if R is None:
+        pytest.skip("reference harness oracle/_ref not built")
+    for name, A in edge_cases():
+        if A.nrow == 0 or A.nrow + A.nnz < 1:
+            continue
+        x = _x(A, dtype)
+        _, y = _run(A, dtype, x)
+        rp, col, v = to_cuda(A, dtype)
+        T, Ln = mb.tile_dims(A.nrow, A.nnz, 14)
+        tx = torch.zeros(T + 1, dtype=torch.int32, device="cuda")
+        ty = torch.zeros(T + 1, dtype=torch.int32, device="cuda")
+        desc = torch.zeros(max(Ln, 1), dtype=torch.int32, device="cuda")
+        assert R.ref_tile_build(14, rp.data_ptr(), A.nrow, A.nnz, tx.data_ptr(), ty.data_ptr(),
+                                desc.data_ptr()) == 0
+        xd = torch.from_numpy(x).cuda()
+        yr = torch.zeros(A.nrow, dtype=XT[dtype], device="cuda")
+        zr = torch.zeros(A.nrow, dtype=XT[dtype], device="cuda")
+        assert R.ref_merbit_spmv(0 if dtype == "f64" else 1, col.data_ptr(), v.data_ptr(),
+                                 A.nrow, A.nnz, tx.data_ptr(), ty.data_ptr(), desc.data_ptr(),
+                                 1.0, xd.data_ptr(), yr.data_ptr(), zr.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        _, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+        e = np.abs(y.astype(np.float64) - yr.cpu().numpy().astype(np.float64))
+        e = e / np.maximum(ya, 1e-300)
+        tol = 1e-12 if dtype == "f64" else 1e-5
+        assert e.max() <= tol, (name, e.max())
+
+
+@pytest.mark.gpu
+def test_full_size_zipf_f64_vs_oracle():
+    """The bench workload itself (Zipf(1.8), 2M rows), against the oracle."""
+    A = synth.workload("zipf_2m")
+    x = synth.uniform(1, A.ncol)
+    _, y = _run(A, "f64", x, tune=True)
+    yo, ya = O.spmm(A.row_ptr, A.col, A.vals, x)
+    emax, emed = O.rel_error(y, yo, ya)
+    assert emax <= TOL["f64"], (emax, emed)
