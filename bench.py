@@ -61,6 +61,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--config", type=int, default=-1,
+                    help="force SpMV kernel configuration index (skips tuning)")
     return ap.parse_args()
 
 
@@ -233,7 +235,9 @@ def run_ours(args):
     xd = torch.from_numpy(x).to(dev).to(xt)
     yd = torch.empty(A.nrow, dtype=xt, device=dev)
     plan = mb.Plan(rp, col, vals, ncol=A.ncol)
-    if not args.no_tune:
+    if args.config >= 0:
+        plan.set_config(args.config)
+    elif not args.no_tune:
         plan.tune(xd)
     info = plan.info()
     B = alg_bytes(A, args.dtype)

@@ -115,6 +115,17 @@ int merbit_plan_set_values(merbit_plan plan, const void* d_vals);
  * Not capturable (it synchronizes). */
 int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream);
 
+/* Kernel configurations the tuner chooses from, for a dtype: kind 0 = CTA
+ * tiles of block*items_per_thread merge items, kind 1 = warp tiles of
+ * 32*items_per_thread items (needs 16-byte aligned row_ptr/col_idx/vals).
+ * merbit_plan_set_config forces one (MERBIT_ERR_INVALID if the plan's
+ * arrays do not allow it); it builds that tile size's partition on first
+ * use, synchronizing `stream`. */
+int merbit_num_configs(merbit_dtype dtype);
+int merbit_config_desc(merbit_dtype dtype, int32_t idx, int32_t* kind, int32_t* block,
+                       int32_t* items_per_thread);
+int merbit_plan_set_config(merbit_plan plan, int32_t idx, void* stream);
+
 /* y[nrow] = alpha*A*x[ncol] + beta*y.  beta == 0 never reads y. */
 int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
                 void* stream);

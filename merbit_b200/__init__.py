@@ -71,6 +71,9 @@ SIGNATURES = {
     "merbit_plan_set_values": (C.c_int, [_P, _P]),
     "merbit_plan_tune": (C.c_int, [_P, _P, _P, _P]),
     "merbit_spmv": (C.c_int, [_P, C.c_double, _P, C.c_double, _P, _P]),
+    "merbit_num_configs": (C.c_int, [C.c_int]),
+    "merbit_config_desc": (C.c_int, [C.c_int, C.c_int32, _P, _P, _P]),
+    "merbit_plan_set_config": (C.c_int, [_P, C.c_int32, _P]),
     "merbit_plan_check": (C.c_int, [_P, _P]),
     "merbit_status_string": (C.c_char_p, [C.c_int]),
     "merbit_last_cuda_error": (C.c_int, []),
@@ -251,6 +254,20 @@ class Plan:
         y = torch.empty(self.nrow, dtype=self.xy_dtype, device=self.device)
         _check(lib().merbit_plan_tune(self._h, _dptr(x), _dptr(y), _stream_ptr(stream)))
         return self.info()
+
+    def configs(self) -> list[tuple[int, int, int, int]]:
+        """[(index, kind, block, items_per_thread)] of the kernel configurations
+        this plan can run (kind 1 needs 16-byte aligned arrays)."""
+        out = []
+        for i in range(lib().merbit_num_configs(self.dtype)):
+            k, b, p = C.c_int32(), C.c_int32(), C.c_int32()
+            _check(lib().merbit_config_desc(self.dtype, i, C.byref(k), C.byref(b), C.byref(p)))
+            if k.value == 0 or self.info().vectorized:
+                out.append((i, k.value, b.value, p.value))
+        return out
+
+    def set_config(self, idx: int, stream=None) -> None:
+        _check(lib().merbit_plan_set_config(self._h, idx, _stream_ptr(stream)))
 
     def check(self, stream=None) -> None:
         """Raise MerbitError if a device-side wait of any launch ran out."""

@@ -50,20 +50,13 @@ int plan_partition(merbit_plan_s* p, int tile_items, const Partition** out, cuda
     int st = build_partition(p->row_ptr, p->nrow, p->nnz, tile_items, &q, s);
     if (st != MERBIT_OK) return st;
     if (q.num_tiles > p->slots) {
-        // grow the carry slots; flags start at 0 which never equals a live
-        // epoch (epochs start at 1 and only increase)
+        // grow the carry slots: both parity arrays start empty (all ones)
         MERBIT_CUDA(cudaStreamSynchronize(s));
-        cudaFree(p->agg);
-        cudaFree(p->flag);
-        p->agg = nullptr;
-        p->flag = nullptr;
-        MERBIT_CUDA(cudaMalloc(&p->agg, sizeof(double) * (size_t)q.num_tiles));
-        MERBIT_CUDA(cudaMalloc(&p->flag, sizeof(unsigned) * (size_t)q.num_tiles));
-        MERBIT_CUDA(cudaMemsetAsync(p->flag, 0, sizeof(unsigned) * (size_t)q.num_tiles, s));
-        // restart epochs so no stale flag can match
-        LaunchState init = {};
-        init.epoch = 1u;
-        MERBIT_CUDA(cudaMemcpyAsync(p->state, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+        cudaFree(p->carry);
+        p->carry = nullptr;
+        const size_t words = 4 * (size_t)q.num_tiles;  // carries + boundary swaps, 2 parities
+        MERBIT_CUDA(cudaMalloc(&p->carry, sizeof(unsigned long long) * words));
+        MERBIT_CUDA(cudaMemsetAsync(p->carry, 0xFF, sizeof(unsigned long long) * words, s));
         MERBIT_CUDA(cudaStreamSynchronize(s));
         p->slots = q.num_tiles;
     }
@@ -76,7 +69,7 @@ int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta
              cudaStream_t s) {
     const SpmvConfig c = spmv_config(p->dtype, cfg);
     const Partition* part = nullptr;
-    int st = plan_partition(p, c.block * c.ipt, &part, s);
+    int st = plan_partition(p, spmv_tile_items(c), &part, s);
     if (st != MERBIT_OK) return st;
     SpmvLaunch a;
     a.row_ptr = p->row_ptr;
@@ -85,9 +78,12 @@ int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta
     a.x = x;
     a.y = y;
     a.coords = part->coords;
-    a.agg = p->agg;
-    a.flag = p->flag;
+    a.slots = p->carry;
+    a.xch = p->carry + 2 * (size_t)p->slots;
+    a.nslots = p->slots;
     a.state = p->state;
+    a.nrow = p->nrow;
+    a.nnz = p->nnz;
     a.num_tiles = part->num_tiles;
     a.alpha = alpha;
     a.beta = beta;
@@ -175,12 +171,14 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
     p->row_ptr = d_row_ptr;
     p->col = d_col_idx;
     p->vals = d_vals;
-    p->vec = aligned16(d_col_idx) && aligned16(d_vals);
+    p->vec = aligned16(d_col_idx) && aligned16(d_vals) && aligned16(d_row_ptr);
     cudaGetDevice(&p->device);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(signature(p));
-        p->cfg = it != g_tune.end() ? it->second : spmv_default_config(dtype, nrow, nnz);
+        p->cfg = it != g_tune.end() && spmv_config_allowed(spmv_config(dtype, it->second), p->vec)
+                     ? it->second
+                     : spmv_default_config(dtype, p->vec);
     }
     cudaError_t e = cudaMalloc(&p->state, sizeof(LaunchState));
     if (e != cudaSuccess) {
@@ -196,7 +194,7 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
     }
     const SpmvConfig c = spmv_config(dtype, p->cfg);
     const Partition* part = nullptr;
-    int st = plan_partition(p, c.block * c.ipt, &part, s);
+    int st = plan_partition(p, spmv_tile_items(c), &part, s);
     if (st == MERBIT_OK) {
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = cuda_fail(e, "plan_create: sync");
@@ -212,8 +210,7 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
 int merbit_plan_destroy(merbit_plan plan) {
     if (!plan) return MERBIT_OK;
     for (auto& q : plan->parts) cudaFree(q.coords);
-    cudaFree(plan->agg);
-    cudaFree(plan->flag);
+    cudaFree(plan->carry);
     cudaFree(plan->state);
     delete plan;
     return MERBIT_OK;
@@ -228,9 +225,9 @@ int merbit_plan_get_info(merbit_plan plan, merbit_plan_info* info) {
     info->dtype = plan->dtype;
     info->block = c.block;
     info->items_per_thread = c.ipt;
-    info->tile_items = c.block * c.ipt;
+    info->tile_items = spmv_tile_items(c);
     info->num_tiles = 0;
-    int64_t meta = sizeof(LaunchState) + (int64_t)plan->slots * (sizeof(double) + sizeof(unsigned));
+    int64_t meta = sizeof(LaunchState) + (int64_t)plan->slots * 4 * (int64_t)sizeof(unsigned long long);
     for (auto& q : plan->parts) {
         if (q.tile_items == info->tile_items) info->num_tiles = q.num_tiles;
         meta += (int64_t)(q.num_tiles + 1) * (int64_t)sizeof(int2);
@@ -247,7 +244,9 @@ int merbit_plan_set_values(merbit_plan plan, const void* d_vals) {
     if (!plan) return fail(MERBIT_ERR_INVALID, "plan_set_values: plan is null");
     if (plan->nnz > 0 && !d_vals) return fail(MERBIT_ERR_INVALID, "plan_set_values: vals is null");
     plan->vals = d_vals;
-    plan->vec = aligned16(plan->col) && aligned16(d_vals);
+    plan->vec = aligned16(plan->col) && aligned16(d_vals) && aligned16(plan->row_ptr);
+    if (!spmv_config_allowed(spmv_config(plan->dtype, plan->cfg), plan->vec))
+        plan->cfg = spmv_default_config(plan->dtype, plan->vec);
     return MERBIT_OK;
 }
 
@@ -272,6 +271,7 @@ int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream)
     float best_ms = 1e30f;
     int st = MERBIT_OK;
     for (int c = 0; c < n && st == MERBIT_OK; ++c) {
+        if (!spmv_config_allowed(spmv_config(plan->dtype, c), plan->vec)) continue;
         for (int w = 0; w < 2 && st == MERBIT_OK; ++w) st = run_spmv(plan, c, 1.0, d_x, 0.0, d_y, s);
         if (st != MERBIT_OK) break;
         const int reps = 5;
@@ -296,6 +296,36 @@ int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream)
     plan->cfg = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[signature(plan)] = best;
+    return MERBIT_OK;
+}
+
+int merbit_num_configs(merbit_dtype dtype) {
+    if (dtype != MERBIT_F64 && dtype != MERBIT_F32 && dtype != MERBIT_BF16) return 0;
+    return spmv_num_configs(dtype);
+}
+
+int merbit_config_desc(merbit_dtype dtype, int32_t idx, int32_t* kind, int32_t* block,
+                       int32_t* items_per_thread) {
+    if (idx < 0 || idx >= merbit_num_configs(dtype) || !kind || !block || !items_per_thread)
+        return fail(MERBIT_ERR_INVALID, "config_desc: bad index");
+    const SpmvConfig c = spmv_config(dtype, idx);
+    *kind = c.kind;
+    *block = c.block;
+    *items_per_thread = c.ipt;
+    return MERBIT_OK;
+}
+
+int merbit_plan_set_config(merbit_plan plan, int32_t idx, void* stream) {
+    if (!plan) return fail(MERBIT_ERR_INVALID, "plan_set_config: plan is null");
+    if (idx < 0 || idx >= spmv_num_configs(plan->dtype))
+        return fail(MERBIT_ERR_INVALID, "plan_set_config: bad index");
+    const SpmvConfig c = spmv_config(plan->dtype, idx);
+    if (!spmv_config_allowed(c, plan->vec))
+        return fail(MERBIT_ERR_INVALID, "plan_set_config: configuration needs 16-byte aligned arrays");
+    const Partition* part = nullptr;
+    int st = plan_partition(plan, spmv_tile_items(c), &part, (cudaStream_t)stream);
+    if (st != MERBIT_OK) return st;
+    plan->cfg = idx;
     return MERBIT_OK;
 }
 

@@ -35,40 +35,74 @@ struct LaunchState {
 // microseconds; the bound only turns a broken invariant into an error code.
 constexpr unsigned long long kCarryWaitNs = 1000000000ull;  // 1 s
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ double ld_relaxed_f64(const double* p) {
-    double v;
-    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
-    return v;
-}
 __device__ __forceinline__ unsigned long long global_timer_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
 
-// Waits until *flag == epoch.  Returns false (and raises MERBIT_ERR_TIMEOUT
-// in st->error) if that takes longer than kCarryWaitNs or another wait of
-// this launch already gave up.
-__device__ __forceinline__ bool wait_epoch(const unsigned* flag, unsigned epoch, LaunchState* st) {
-    if (ld_acquire_u32(flag) == epoch) return true;
-    const unsigned long long t0 = global_timer_ns();
+// ---- shared-memory barriers and bulk (TMA) copies, sm_90+ ----------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+// Makes an initialized mbarrier visible to the async (bulk copy) proxy.
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// L2 policy: streamed matrix data is evicted first so that x stays in L2.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+// Bulk global->shared copy completing on `bar`; dst, src 16-byte aligned,
+// bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar,
+                                         uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
+        "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+// Waits for phase `phase` of `bar` for at most kCarryWaitNs; on time-out
+// raises MERBIT_ERR_TIMEOUT, waits once more (bounded) for the copies still
+// in flight, and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase,
+                                                  LaunchState* st) {
+    if (mbar_try_wait(bar, phase)) return true;
+    unsigned long long t0 = global_timer_ns();
     for (;;) {
-        __nanosleep(64);
-        if (ld_acquire_u32(flag) == epoch) return true;
-        if (*(volatile int*)&st->error != 0) return false;
-        if (global_timer_ns() - t0 > kCarryWaitNs) {
-            atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
-            return false;
-        }
+        if (mbar_try_wait(bar, phase)) return true;
+        if (global_timer_ns() - t0 > kCarryWaitNs) break;
     }
+    atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
+    t0 = global_timer_ns();
+    while (!mbar_try_wait(bar, phase) && global_timer_ns() - t0 < kCarryWaitNs) {
+    }
+    return false;
 }
 
 // Draws this CTA's tile (thread 0 only) and the launch epoch.
@@ -87,6 +121,87 @@ __device__ __forceinline__ void finish_launch(LaunchState* st, unsigned epoch) {
         __threadfence();
         *(volatile unsigned*)&st->epoch = epoch + 1u;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Carry slots.  Two arrays of nslots 8-byte words, selected by the parity of
+// the launch epoch.  A tile publishes its trailing partial sum as one word in
+// the current array; a reader spins until the word is no longer kEmpty, so
+// one load returns both "ready" and the value.  Every launch refills the
+// other array with kEmpty, which makes it ready for the next launch whatever
+// tiles this one used (CUDA-graph replays included).  A value whose bits
+// happen to equal kEmpty (a NaN) is published as the canonical NaN.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kEmpty = ~0ull;
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void publish_carry(unsigned long long* slots, int nslots,
+                                              unsigned epoch, int t, double v) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    if (b == kEmpty) b = 0x7FF8000000000000ull;
+    st_relaxed_u64(slots + (size_t)(epoch & 1u) * nslots + t, b);
+}
+
+// Reads tile t's carry, waiting (bounded) until it is published.
+__device__ __forceinline__ double read_carry(const unsigned long long* slots, int nslots,
+                                             unsigned epoch, int t, LaunchState* st) {
+    const unsigned long long* p = slots + (size_t)(epoch & 1u) * nslots + t;
+    unsigned long long b = ld_relaxed_u64(p);
+    if (b != kEmpty) return __longlong_as_double((long long)b);
+    const unsigned long long t0 = global_timer_ns();
+    for (;;) {
+        __nanosleep(32);
+        b = ld_relaxed_u64(p);
+        if (b != kEmpty) return __longlong_as_double((long long)b);
+        if (*(volatile int*)&st->error != 0) return 0.0;
+        if (global_timer_ns() - t0 > kCarryWaitNs) {
+            atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
+            return 0.0;
+        }
+    }
+}
+
+// Grid-strided refill of the other parity's slots.
+__device__ __forceinline__ void reset_other_parity(unsigned long long* slots, int nslots,
+                                                   unsigned epoch) {
+    unsigned long long* o = slots + (size_t)((epoch + 1u) & 1u) * nslots;
+    const int stride = (int)(gridDim.x * blockDim.x);
+    for (int i = (int)(blockIdx.x * blockDim.x + threadIdx.x); i < nslots; i += stride)
+        o[i] = kEmpty;
+}
+
+// Decoupled look-back by one warp: the sum of the carries of tiles u-1,
+// u-2, ... down to the tile that contains nonzero index rs (the start of
+// the row that tile u completes first), in a fixed order -- 32 tiles per
+// step, butterfly reduction -- so the result does not depend on timing.
+__device__ __forceinline__ double look_back(const int2* coords, const unsigned long long* slots,
+                                            int nslots, unsigned epoch, LaunchState* st, int u,
+                                            int rs, int lane) {
+    double total = 0.0;
+    int base = u - 1;
+    for (;;) {
+        const int tq = base - lane;
+        const bool valid = tq >= 0;
+        const int cx = valid ? coords[tq].x : 0;
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, !valid || cx <= rs);
+        const int last = m ? __ffs(m) - 1 : 31;
+        double c = 0.0;
+        if (valid && lane <= last) c = read_carry(slots, nslots, epoch, tq, st);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+        total += c;
+        if (m) break;
+        base -= 32;
+    }
+    return total;
 }
 
 // ---------------------------------------------------------------------------
@@ -214,12 +329,16 @@ int build_partition(const int32_t* row_ptr, int nrow, int nnz, int tile_items, P
 
 // SpMV kernel configurations (spmv.cu).
 struct SpmvConfig {
+    int kind;  // 0: CTA-tile kernel, 1: warp-tile kernel
     int block;
     int ipt;
+    int stages;  // warp-tile kernel: shared-memory stages per warp (1 or 2)
 };
 int spmv_num_configs(int dtype);
 SpmvConfig spmv_config(int dtype, int idx);
-int spmv_default_config(int dtype, int nrow, int nnz);
+int spmv_tile_items(const SpmvConfig& c);
+bool spmv_config_allowed(const SpmvConfig& c, bool vec);
+int spmv_default_config(int dtype, bool vec);
 
 struct SpmvLaunch {
     const int32_t* row_ptr;
@@ -228,10 +347,12 @@ struct SpmvLaunch {
     const void* x;
     void* y;
     const int2* coords;
-    double* agg;
-    unsigned* flag;
+    unsigned long long* slots;  // 2 * nslots carry slots (see publish_carry)
+    unsigned long long* xch;    // 2 * nslots boundary-swap slots (warp-tile kernel)
     LaunchState* state;
+    int nrow, nnz;
     int num_tiles;
+    int nslots;
     double alpha, beta;
 };
 int spmv_launch(int dtype, int cfg, bool vec, const SpmvLaunch& a, cudaStream_t s);
@@ -248,10 +369,9 @@ struct merbit_plan_s {
     int device = 0;
     int cfg = 0;  // index into the SpMV config table
     std::vector<merbit::Partition> parts;
-    // carry slots shared by every launch of this plan (sized for the
-    // largest tile count in use)
-    double* agg = nullptr;
-    unsigned* flag = nullptr;
+    // carry slots shared by every launch of this plan (2 * slots words,
+    // sized for the largest tile count in use)
+    unsigned long long* carry = nullptr;
     int slots = 0;
     merbit::LaunchState* state = nullptr;
 };

@@ -64,6 +64,8 @@ __global__ void __launch_bounds__(BLOCK) spmv_tile_kernel(const SpmvLaunch a) {
     __syncthreads();
     const int t = s_tile;
     const unsigned epoch = s_epoch;
+    reset_other_parity(a.slots, a.nslots, epoch);
+    reset_other_parity(a.xch, a.nslots, epoch);
     if (t >= a.num_tiles) {  // launch bookkeeping out of step: report, touch nothing
         if (tid == 0) {
             atomicExch(&a.state->error, (int)MERBIT_ERR_TIMEOUT);
@@ -218,11 +220,7 @@ __global__ void __launch_bounds__(BLOCK) spmv_tile_kernel(const SpmvLaunch a) {
     if (has_end) s_rows[first_row] = excl + first_val;
 
     // ---- publish this tile's carry: the partial sum of its trailing row
-    if (tid == BLOCK - 1) {
-        const double tot = f ? v : pv + v;
-        a.agg[t] = tot;
-        st_release_u32(a.flag + t, epoch);
-    }
+    if (tid == BLOCK - 1) publish_carry(a.slots, a.nslots, epoch, t, f ? v : pv + v);
 
     // ---- decoupled look-back for the tile's first row when it began in an
     // earlier tile and ends here.  Earlier tiles are summed in a fixed order
@@ -230,25 +228,7 @@ __global__ void __launch_bounds__(BLOCK) spmv_tile_kernel(const SpmvLaunch a) {
     // timing.
     const bool need_lb = nr > 0 && s_rp[0] < x0;
     if (need_lb && warp == 0) {
-        const int rs = s_rp[0];
-        double total = 0.0;
-        int base = t - 1;
-        for (;;) {
-            const int tq = base - lane;
-            const bool valid = tq >= 0;
-            const int cx = valid ? a.coords[tq].x : 0;
-            const unsigned m = __ballot_sync(0xFFFFFFFFu, !valid || cx <= rs);
-            const int last = m ? __ffs(m) - 1 : 31;
-            double c = 0.0;
-            if (valid && lane <= last) {
-                if (wait_epoch(a.flag + tq, epoch, a.state)) c = ld_relaxed_f64(a.agg + tq);
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
-            total += c;
-            if (m) break;
-            base -= 32;
-        }
+        const double total = look_back(a.coords, a.slots, a.nslots, epoch, a.state, t, s_rp[0], lane);
         if (lane == 0) s_carry = total;
     }
     __syncthreads();
@@ -267,11 +247,21 @@ __global__ void __launch_bounds__(BLOCK) spmv_tile_kernel(const SpmvLaunch a) {
 }
 
 // ---------------------------------------------------------------------------
-// Configuration table.  Items per tile = block * ipt.
+// Configuration table.  kind 0 = this CTA-tile kernel (tile = block*ipt
+// items), kind 1 = the warp-tile kernel of spmv_warp.cu (tile = 32*ipt items,
+// block/32 warps per CTA, needs 16-byte aligned col_idx/vals).
 // ---------------------------------------------------------------------------
 namespace {
-constexpr SpmvConfig kCfgF64[] = {{256, 8}, {256, 6}, {128, 8}, {256, 12}};
-constexpr SpmvConfig kCfgF32[] = {{256, 12}, {256, 8}, {256, 16}, {128, 12}};
+// Items per thread are odd: a lane's segment then starts an odd number of
+// elements after its neighbour's, which spreads the lanes of a warp over
+// all shared-memory banks when they walk their segments in step.
+// stages: shared-memory stages per warp of the warp-tile kernel (1 or 2).
+constexpr SpmvConfig kCfgF64[] = {
+    {1, 256, 15, 1}, {1, 128, 15, 1}, {1, 256, 11, 1}, {1, 256, 7, 1}, {1, 128, 23, 1},
+    {1, 128, 15, 2}, {1, 128, 7, 2},  {0, 256, 7, 1},  {0, 256, 11, 1}, {0, 128, 9, 1}};
+constexpr SpmvConfig kCfgF32[] = {
+    {1, 256, 15, 1}, {1, 128, 15, 1}, {1, 256, 11, 1}, {1, 256, 7, 1}, {1, 128, 23, 1},
+    {1, 128, 15, 2}, {1, 128, 7, 2},  {0, 256, 11, 1}, {0, 256, 7, 1},  {0, 256, 15, 1}};
 
 template <int DT, int BLOCK, int IPT, bool VEC>
 int launch_one(const SpmvLaunch& a, cudaStream_t s) {
@@ -296,6 +286,17 @@ template <int DT, int BLOCK, int IPT>
 int launch_vec(bool vec, const SpmvLaunch& a, cudaStream_t s) {
     return vec ? launch_one<DT, BLOCK, IPT, true>(a, s) : launch_one<DT, BLOCK, IPT, false>(a, s);
 }
+
+template <int DT>
+int launch_cta(int block, int ipt, bool vec, const SpmvLaunch& a, cudaStream_t s) {
+    if (block == 256 && ipt == 7) return launch_vec<DT, 256, 7>(vec, a, s);
+    if (block == 256 && ipt == 11) return launch_vec<DT, 256, 11>(vec, a, s);
+    if (block == 128 && ipt == 9) return launch_vec<DT, 128, 9>(vec, a, s);
+    if (block == 256 && ipt == 5) return launch_vec<DT, 256, 5>(vec, a, s);
+    if (block == 256 && ipt == 15) return launch_vec<DT, 256, 15>(vec, a, s);
+    if (block == 128 && ipt == 11) return launch_vec<DT, 128, 11>(vec, a, s);
+    return fail(MERBIT_ERR_INVALID, "spmv: no such configuration");
+}
 }  // namespace
 
 int spmv_num_configs(int dtype) {
@@ -307,42 +308,31 @@ SpmvConfig spmv_config(int dtype, int idx) {
     return dtype == MERBIT_F64 ? kCfgF64[idx] : kCfgF32[idx];
 }
 
-int spmv_default_config(int dtype, int nrow, int nnz) {
-    (void)nrow;
-    (void)nnz;
-    (void)dtype;
+int spmv_tile_items(const SpmvConfig& c) { return c.kind == 1 ? 32 * c.ipt : c.block * c.ipt; }
+
+bool spmv_config_allowed(const SpmvConfig& c, bool vec) { return vec || c.kind == 0; }
+
+int spmv_default_config(int dtype, bool vec) {
+    const int n = spmv_num_configs(dtype);
+    for (int i = 0; i < n; ++i)
+        if (spmv_config_allowed(spmv_config(dtype, i), vec)) return i;
     return 0;
 }
 
+int spmv_warp_launch(int dtype, int warps, int ipt, int stages, const SpmvLaunch& a,
+                     cudaStream_t s);
+
 int spmv_launch(int dtype, int cfg, bool vec, const SpmvLaunch& a, cudaStream_t s) {
     if (a.num_tiles <= 0) return MERBIT_OK;
+    const SpmvConfig c = spmv_config(dtype, cfg);
+    if (!spmv_config_allowed(c, vec)) return fail(MERBIT_ERR_INVALID, "spmv: config needs aligned arrays");
+    if (c.kind == 1) return spmv_warp_launch(dtype, c.block / 32, c.ipt, c.stages, a, s);
     switch (dtype) {
-    case MERBIT_F64:
-        switch (cfg) {
-        case 0: return launch_vec<MERBIT_F64, 256, 8>(vec, a, s);
-        case 1: return launch_vec<MERBIT_F64, 256, 6>(vec, a, s);
-        case 2: return launch_vec<MERBIT_F64, 128, 8>(vec, a, s);
-        case 3: return launch_vec<MERBIT_F64, 256, 12>(vec, a, s);
-        }
-        break;
-    case MERBIT_F32:
-        switch (cfg) {
-        case 0: return launch_vec<MERBIT_F32, 256, 12>(vec, a, s);
-        case 1: return launch_vec<MERBIT_F32, 256, 8>(vec, a, s);
-        case 2: return launch_vec<MERBIT_F32, 256, 16>(vec, a, s);
-        case 3: return launch_vec<MERBIT_F32, 128, 12>(vec, a, s);
-        }
-        break;
-    case MERBIT_BF16:
-        switch (cfg) {
-        case 0: return launch_vec<MERBIT_BF16, 256, 12>(vec, a, s);
-        case 1: return launch_vec<MERBIT_BF16, 256, 8>(vec, a, s);
-        case 2: return launch_vec<MERBIT_BF16, 256, 16>(vec, a, s);
-        case 3: return launch_vec<MERBIT_BF16, 128, 12>(vec, a, s);
-        }
-        break;
+    case MERBIT_F64: return launch_cta<MERBIT_F64>(c.block, c.ipt, vec, a, s);
+    case MERBIT_F32: return launch_cta<MERBIT_F32>(c.block, c.ipt, vec, a, s);
+    case MERBIT_BF16: return launch_cta<MERBIT_BF16>(c.block, c.ipt, vec, a, s);
     }
-    return fail(MERBIT_ERR_INVALID, "spmv: bad dtype/config");
+    return fail(MERBIT_ERR_INVALID, "spmv: bad dtype");
 }
 
 }  // namespace merbit

@@ -55,15 +55,26 @@ def test_spmv_vs_oracle(name, A, dtype):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
-def test_spmv_every_config(dtype):
+@pytest.mark.parametrize("workload", ["zipf_small", "laplace2d_small", "stencil27_small"])
+def test_spmv_every_config(dtype, workload):
     """Every tile configuration the tuner can pick gives the oracle's answer."""
-    A = synth.workload("zipf_small")
+    A = synth.workload(workload)
     x = _x(A, dtype)
     yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
     rp, col, v = to_cuda(A, dtype)
     plan = mb.Plan(rp, col, v)
-    plan.tune(torch.from_numpy(x).cuda())
-    y = plan.spmv(torch.from_numpy(x).cuda())
+    xd = torch.from_numpy(x).cuda()
+    cfgs = plan.configs()
+    assert any(k == 1 for _, k, _, _ in cfgs) and any(k == 0 for _, k, _, _ in cfgs)
+    for idx, kind, block, ipt in cfgs:
+        plan.set_config(idx)
+        assert plan.info().tile_items == (32 * ipt if kind == 1 else block * ipt)
+        y = plan.spmv(xd)
+        torch.cuda.synchronize()
+        plan.check()
+        assert O.rel_error(y.cpu().numpy(), yo, ya)[0] <= TOL[dtype], (idx, kind, block, ipt)
+    plan.tune(xd)
+    y = plan.spmv(xd)
     assert O.rel_error(y.cpu().numpy(), yo, ya)[0] <= TOL[dtype]
 
 
@@ -204,3 +215,26 @@ def test_full_size_zipf_f64_vs_oracle():
     yo, ya = O.spmm(A.row_ptr, A.col, A.vals, x)
     emax, emed = O.rel_error(y, yo, ya)
     assert emax <= TOL["f64"], (emax, emed)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_alternating_kernels_share_carry_slots(dtype):
+    """Launches that alternate between kernel kinds and tile sizes on one
+    plan (as the tuner does) must each see clean carry / swap slots."""
+    A = synth.workload("zipf_small")
+    x = _x(A, dtype)
+    yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+    rp, col, v = to_cuda(A, dtype)
+    plan = mb.Plan(rp, col, v)
+    xd = torch.from_numpy(x).cuda()
+    cfgs = plan.configs()
+    warp = [c[0] for c in cfgs if c[1] == 1]
+    cta = [c[0] for c in cfgs if c[1] == 0]
+    order = [warp[0], cta[0], warp[0], warp[1], cta[1], cta[0], warp[0], warp[-1], cta[-1], warp[0]]
+    for idx in order * 2:
+        plan.set_config(idx)
+        y = plan.spmv(xd)
+        torch.cuda.synchronize()
+        assert O.rel_error(y.cpu().numpy(), yo, ya)[0] <= TOL[dtype], idx
+    plan.check()
