@@ -125,6 +125,8 @@ int merbit_num_configs(merbit_dtype dtype);
 int merbit_config_desc(merbit_dtype dtype, int32_t idx, int32_t* kind, int32_t* block,
                        int32_t* items_per_thread);
 int merbit_plan_set_config(merbit_plan plan, int32_t idx, void* stream);
+/* *usable = 1 when configuration idx can run this plan (same rules). */
+int merbit_plan_config_usable(merbit_plan plan, int32_t idx, int32_t* usable, void* stream);
 
 /* y[nrow] = alpha*A*x[ncol] + beta*y.  beta == 0 never reads y. */
 int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,

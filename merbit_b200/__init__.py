@@ -74,6 +74,7 @@ SIGNATURES = {
     "merbit_num_configs": (C.c_int, [C.c_int]),
     "merbit_config_desc": (C.c_int, [C.c_int, C.c_int32, _P, _P, _P]),
     "merbit_plan_set_config": (C.c_int, [_P, C.c_int32, _P]),
+    "merbit_plan_config_usable": (C.c_int, [_P, C.c_int32, _P, _P]),
     "merbit_plan_check": (C.c_int, [_P, _P]),
     "merbit_status_string": (C.c_char_p, [C.c_int]),
     "merbit_last_cuda_error": (C.c_int, []),
@@ -260,9 +261,10 @@ class Plan:
         this plan can run (kind 1 needs 16-byte aligned arrays)."""
         out = []
         for i in range(lib().merbit_num_configs(self.dtype)):
-            k, b, p = C.c_int32(), C.c_int32(), C.c_int32()
+            k, b, p, ok = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
             _check(lib().merbit_config_desc(self.dtype, i, C.byref(k), C.byref(b), C.byref(p)))
-            if k.value == 0 or self.info().vectorized:
+            _check(lib().merbit_plan_config_usable(self._h, i, C.byref(ok), _stream_ptr(None)))
+            if ok.value:
                 out.append((i, k.value, b.value, p.value))
         return out
 

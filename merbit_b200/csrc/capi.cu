@@ -65,6 +65,33 @@ int plan_partition(merbit_plan_s* p, int tile_items, const Partition** out, cuda
     return MERBIT_OK;
 }
 
+// Whether configuration idx can run this plan (builds its partition).
+int plan_config_ok(merbit_plan_s* p, int idx, bool* ok, cudaStream_t s) {
+    *ok = false;
+    const SpmvConfig c = spmv_config(p->dtype, idx);
+    if (!spmv_config_allowed(c, p->vec)) return MERBIT_OK;
+    const Partition* part = nullptr;
+    int st = plan_partition(p, spmv_tile_items(c), &part, s);
+    if (st != MERBIT_OK) return st;
+    *ok = part->max_rows <= spmv_config_row_cap(c);
+    return MERBIT_OK;
+}
+
+// First usable configuration in table order.
+int plan_pick_default(merbit_plan_s* p, cudaStream_t s) {
+    const int n = spmv_num_configs(p->dtype);
+    for (int i = 0; i < n; ++i) {
+        bool ok = false;
+        int st = plan_config_ok(p, i, &ok, s);
+        if (st != MERBIT_OK) return st;
+        if (ok) {
+            p->cfg = i;
+            return MERBIT_OK;
+        }
+    }
+    return fail(MERBIT_ERR_UNSUPPORTED, "no SpMV configuration fits this matrix");
+}
+
 int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta, void* y,
              cudaStream_t s) {
     const SpmvConfig c = spmv_config(p->dtype, cfg);
@@ -173,12 +200,11 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
     p->vals = d_vals;
     p->vec = aligned16(d_col_idx) && aligned16(d_vals) && aligned16(d_row_ptr);
     cudaGetDevice(&p->device);
+    int tuned = -1;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(signature(p));
-        p->cfg = it != g_tune.end() && spmv_config_allowed(spmv_config(dtype, it->second), p->vec)
-                     ? it->second
-                     : spmv_default_config(dtype, p->vec);
+        if (it != g_tune.end()) tuned = it->second;
     }
     cudaError_t e = cudaMalloc(&p->state, sizeof(LaunchState));
     if (e != cudaSuccess) {
@@ -192,9 +218,15 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
         merbit_plan_destroy(p);
         return cuda_fail(e, "plan_create: init state");
     }
-    const SpmvConfig c = spmv_config(dtype, p->cfg);
-    const Partition* part = nullptr;
-    int st = plan_partition(p, spmv_tile_items(c), &part, s);
+    int st = MERBIT_OK;
+    bool tuned_ok = false;
+    if (tuned >= 0) st = plan_config_ok(p, tuned, &tuned_ok, s);
+    if (st == MERBIT_OK) {
+        if (tuned_ok)
+            p->cfg = tuned;
+        else
+            st = plan_pick_default(p, s);
+    }
     if (st == MERBIT_OK) {
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = cuda_fail(e, "plan_create: sync");
@@ -245,9 +277,10 @@ int merbit_plan_set_values(merbit_plan plan, const void* d_vals) {
     if (plan->nnz > 0 && !d_vals) return fail(MERBIT_ERR_INVALID, "plan_set_values: vals is null");
     plan->vals = d_vals;
     plan->vec = aligned16(plan->col) && aligned16(d_vals) && aligned16(plan->row_ptr);
-    if (!spmv_config_allowed(spmv_config(plan->dtype, plan->cfg), plan->vec))
-        plan->cfg = spmv_default_config(plan->dtype, plan->vec);
-    return MERBIT_OK;
+    bool ok = false;
+    int st = plan_config_ok(plan, plan->cfg, &ok, nullptr);
+    if (st == MERBIT_OK && !ok) st = plan_pick_default(plan, nullptr);
+    return st;
 }
 
 int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
@@ -271,7 +304,10 @@ int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream)
     float best_ms = 1e30f;
     int st = MERBIT_OK;
     for (int c = 0; c < n && st == MERBIT_OK; ++c) {
-        if (!spmv_config_allowed(spmv_config(plan->dtype, c), plan->vec)) continue;
+        bool ok = false;
+        st = plan_config_ok(plan, c, &ok, s);
+        if (st != MERBIT_OK) break;
+        if (!ok) continue;
         for (int w = 0; w < 2 && st == MERBIT_OK; ++w) st = run_spmv(plan, c, 1.0, d_x, 0.0, d_y, s);
         if (st != MERBIT_OK) break;
         const int reps = 5;
@@ -319,14 +355,25 @@ int merbit_plan_set_config(merbit_plan plan, int32_t idx, void* stream) {
     if (!plan) return fail(MERBIT_ERR_INVALID, "plan_set_config: plan is null");
     if (idx < 0 || idx >= spmv_num_configs(plan->dtype))
         return fail(MERBIT_ERR_INVALID, "plan_set_config: bad index");
-    const SpmvConfig c = spmv_config(plan->dtype, idx);
-    if (!spmv_config_allowed(c, plan->vec))
-        return fail(MERBIT_ERR_INVALID, "plan_set_config: configuration needs 16-byte aligned arrays");
-    const Partition* part = nullptr;
-    int st = plan_partition(plan, spmv_tile_items(c), &part, (cudaStream_t)stream);
+    bool ok = false;
+    int st = plan_config_ok(plan, idx, &ok, (cudaStream_t)stream);
     if (st != MERBIT_OK) return st;
+    if (!ok)
+        return fail(MERBIT_ERR_INVALID,
+                    "plan_set_config: configuration cannot run this plan (needs 16-byte aligned "
+                    "arrays, or the matrix ends too many rows in one tile)");
     plan->cfg = idx;
     return MERBIT_OK;
+}
+
+int merbit_plan_config_usable(merbit_plan plan, int32_t idx, int32_t* usable, void* stream) {
+    if (!plan || !usable) return fail(MERBIT_ERR_INVALID, "plan_config_usable: null pointer");
+    if (idx < 0 || idx >= spmv_num_configs(plan->dtype))
+        return fail(MERBIT_ERR_INVALID, "plan_config_usable: bad index");
+    bool ok = false;
+    int st = plan_config_ok(plan, idx, &ok, (cudaStream_t)stream);
+    *usable = ok ? 1 : 0;
+    return st;
 }
 
 int merbit_plan_check(merbit_plan plan, void* stream) {

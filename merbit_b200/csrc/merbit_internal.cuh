@@ -321,8 +321,14 @@ inline size_t xy_size(int dt) { return dt == MERBIT_F64 ? 8 : 4; }
 struct Partition {
     int tile_items = 0;
     int num_tiles = 0;
+    int max_rows = 0;  // largest number of row ends in one tile
     int2* coords = nullptr;
 };
+
+// Entries of the row_ptr window a warp-tile stage holds (32*ipt merge items
+// per tile); a plan whose tiles end more than warp_rp_cap(ipt) - 8 rows
+// cannot use that configuration.
+constexpr int warp_rp_cap(int ipt) { return (32 * ipt) / 3 + 16; }
 
 int build_partition(const int32_t* row_ptr, int nrow, int nnz, int tile_items, Partition* out,
                     cudaStream_t s);
@@ -338,7 +344,7 @@ int spmv_num_configs(int dtype);
 SpmvConfig spmv_config(int dtype, int idx);
 int spmv_tile_items(const SpmvConfig& c);
 bool spmv_config_allowed(const SpmvConfig& c, bool vec);
-int spmv_default_config(int dtype, bool vec);
+int spmv_config_row_cap(const SpmvConfig& c);
 
 struct SpmvLaunch {
     const int32_t* row_ptr;

@@ -124,6 +124,16 @@ __global__ void validate_kernel(const int32_t* __restrict__ row_ptr,
     }
 }
 
+__global__ void max_rows_kernel(const int2* __restrict__ coords, int num_tiles,
+                                int* __restrict__ out) {
+    int m = 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles;
+         t += gridDim.x * blockDim.x)
+        m = max(m, coords[t + 1].y - coords[t].y);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 int build_partition(const int32_t* row_ptr, int nrow, int nnz, int tile_items, Partition* out,
                     cudaStream_t s) {
     const long long total = (long long)nrow + nnz;
@@ -138,6 +148,21 @@ int build_partition(const int32_t* row_ptr, int nrow, int nnz, int tile_items, P
     merge_coords_kernel<<<grid, bs, 0, s>>>(row_ptr, nrow, nnz, tile_items, count, nullptr,
                                             nullptr, out->coords);
     MERBIT_CUDA(cudaGetLastError());
+    // largest rows-per-tile, which decides the configurations the plan can use
+    int* d_max = nullptr;
+    MERBIT_CUDA(cudaMalloc(&d_max, sizeof(int)));
+    int h_max = 0;
+    cudaError_t e = cudaMemsetAsync(d_max, 0, sizeof(int), s);
+    if (e == cudaSuccess && T > 0) {
+        max_rows_kernel<<<(unsigned)min((T + 255) / 256, 1024LL), 256, 0, s>>>(out->coords, (int)T,
+                                                                               d_max);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_max, d_max, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_max);
+    if (e != cudaSuccess) return cuda_fail(e, "build_partition: max rows");
+    out->max_rows = h_max;
     return MERBIT_OK;
 }
 

@@ -312,12 +312,10 @@ int spmv_tile_items(const SpmvConfig& c) { return c.kind == 1 ? 32 * c.ipt : c.b
 
 bool spmv_config_allowed(const SpmvConfig& c, bool vec) { return vec || c.kind == 0; }
 
-int spmv_default_config(int dtype, bool vec) {
-    const int n = spmv_num_configs(dtype);
-    for (int i = 0; i < n; ++i)
-        if (spmv_config_allowed(spmv_config(dtype, i), vec)) return i;
-    return 0;
+int spmv_config_row_cap(const SpmvConfig& c) {
+    return c.kind == 1 ? warp_rp_cap(c.ipt) - 8 : INT_MAX;
 }
+
 
 int spmv_warp_launch(int dtype, int warps, int ipt, int stages, const SpmvLaunch& a,
                      cudaStream_t s);

@@ -45,19 +45,24 @@ namespace merbit {
 
 constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
-// Rows of one tile staged for the coalesced write; rows beyond are stored
-// directly.
-constexpr int kOutCap = 128;
-
-template <typename V, int IPT>
+// One stage of a warp: row_ptr window (warp_rp_cap entries: the plan only
+// runs this configuration when no tile ends more rows than fit), col slice
+// and value slice (W + rounding), one mbarrier.  Completed rows are staged
+// for the coalesced write in whichever slice is dead after the products are
+// formed: the col slice when products overwrite the values, the value slice
+// when they overwrite the columns (bf16); rows beyond OUTCAP go straight to y.
+template <typename V, typename P, int IPT>
 struct WarpSmem {
     static constexpr int W = 32 * IPT;
-    static constexpr int CAP = W + 32;  // window + rounding on both sides
-    static constexpr size_t rp_bytes = align16((size_t)CAP * 4);
+    static constexpr int CAP = W + 32;  // slice + rounding on both sides
+    static constexpr size_t rp_bytes = align16((size_t)warp_rp_cap(IPT) * 4);
     static constexpr size_t col_bytes = align16((size_t)CAP * 4);
     static constexpr size_t val_bytes = align16((size_t)CAP * sizeof(V));
-    static constexpr size_t out_offset = rp_bytes + col_bytes + val_bytes;
-    static constexpr size_t bar_offset = out_offset + (size_t)kOutCap * 8;
+    static constexpr bool prod_in_val = sizeof(P) == sizeof(V);
+    static constexpr size_t out_offset = prod_in_val ? rp_bytes : rp_bytes + col_bytes;
+    static constexpr int OUTCAP_ = (int)((prod_in_val ? col_bytes : val_bytes) / 8);
+    static constexpr int OUTCAP = OUTCAP_ < 256 ? OUTCAP_ : 256;
+    static constexpr size_t bar_offset = rp_bytes + col_bytes + val_bytes;
     static constexpr size_t bytes = bar_offset + 16;
 };
 
@@ -133,8 +138,9 @@ struct WarpTile {
     using Y = typename Pr::Y;
     using P = typename Pr::P;
     using Acc = typename Pr::Acc;
-    using S = WarpSmem<V, IPT>;
+    using S = WarpSmem<V, P, IPT>;
     static constexpr int GV = 16 / (int)sizeof(V);
+    static constexpr int kOutCap = S::OUTCAP;
 
     // Issues the copies of tile u into stage `ws`; lane 0 arms the barrier
     // with the byte count before any copy is issued.
@@ -394,7 +400,7 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch 
 namespace {
 template <int DT, int WARPS, int IPT, int STAGES>
 int launch_warp(const SpmvLaunch& a, cudaStream_t s) {
-    using S = WarpSmem<typename Prec<DT>::V, IPT>;
+    using S = WarpSmem<typename Prec<DT>::V, typename Prec<DT>::P, IPT>;
     constexpr size_t smem = S::bytes * WARPS * STAGES;
     static int grid_cap[64] = {};  // resident CTAs per device, from the occupancy calculator
     int dev = 0;
