@@ -132,6 +132,28 @@ int merbit_plan_config_usable(merbit_plan plan, int32_t idx, int32_t* usable, vo
 int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
                 void* stream);
 
+/* y[nrow] = alpha*A*x + beta*y without allocating any device memory -- for
+ * callers that cannot allocate on the call path: code running while a CUDA
+ * stream is captured (cudaMalloc cannot be captured), hosts whose device
+ * memory all belongs to their own pool allocator, and loops that cannot
+ * afford cudaMalloc's implicit synchronization.  No counterpart in the
+ * reference.
+ *
+ * Its scratch (tile coordinates, carry slots, launch counters) is one fixed
+ * file-scope device array of about 1.3 MB, held by every GPU that loads the
+ * library until the process exits.  It bounds the matrix: nrow + nnz <=
+ * 58,720,256 (32,768 tiles of 1,792 merge items); larger matrices are
+ * rejected with MERBIT_ERR_INVALID -- use merbit_plan_create/merbit_spmv.
+ * The caller passes all arrays (device pointers, same dtype rules as a
+ * plan).  The structure is not validated: it must be valid CSR.  The first
+ * call on a device looks the array up and initializes it on `stream`; make
+ * that first call before any stream capture.  Every call reuses the same
+ * array (each call rebuilds what it needs), so calls whose executions
+ * overlap on the GPU -- on different streams without ordering -- race. */
+int merbit_spmv_noalloc(int32_t nrow, int32_t ncol, int32_t nnz, const int32_t* d_row_ptr,
+                        const int32_t* d_col_idx, const void* d_vals, merbit_dtype dtype,
+                        double alpha, const void* d_x, double beta, void* d_y, void* stream);
+
 /* Reads and clears the plan's device-side status (MERBIT_ERR_TIMEOUT if a
  * carry wait ran out in any launch since the last check).  Synchronizes. */
 int merbit_plan_check(merbit_plan plan, void* stream);

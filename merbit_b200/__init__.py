@@ -76,6 +76,8 @@ SIGNATURES = {
     "merbit_plan_set_config": (C.c_int, [_P, C.c_int32, _P]),
     "merbit_plan_config_usable": (C.c_int, [_P, C.c_int32, _P, _P]),
     "merbit_plan_check": (C.c_int, [_P, _P]),
+    "merbit_spmv_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int,
+                                      C.c_double, _P, C.c_double, _P, _P]),
     "merbit_status_string": (C.c_char_p, [C.c_int]),
     "merbit_last_cuda_error": (C.c_int, []),
     "merbit_last_error_detail": (C.c_char_p, []),
