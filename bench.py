@@ -332,7 +332,8 @@ def run_ours(args):
             "l2": "inputs larger than L2 (matrix streamed from HBM every step); "
                   "value_l2_flushed flushes L2 before every launch",
             "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-            "kernel": f"spmv_tile_kernel block={info.block} ipt={info.items_per_thread} "
+            "kernel": f"{'spmv_warp_kernel' if info.kind == 1 else 'spmv_tile_kernel'} "
+                      f"block={info.block} ipt={info.items_per_thread} "
                       f"tile_items={info.tile_items} tiles={info.num_tiles} "
                       f"vectorized={int(info.vectorized)}",
         },
@@ -350,7 +351,7 @@ def run_ours(args):
             "frac": round(achieved / peak, 4),
             "peak_source": f"{peak_src} hbm_gbs (copy), burst",
             "traffic": traffic,
-            "kernel": "spmv_tile_kernel",
+            "kernel": "spmv_warp_kernel" if info.kind == 1 else "spmv_tile_kernel",
         },
         "e2e": {
             "value": round(ws * B / (ms_e2e * 1e-3) / 1e9, 2),

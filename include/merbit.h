@@ -70,6 +70,7 @@ typedef struct merbit_plan_info {
     int32_t tile_items;      /* merge items (row ends + nonzeros) per tile */
     int32_t num_tiles;
     int32_t vectorized;      /* 1 when 128-bit loads of col_idx/vals are used */
+    int32_t kind;            /* 0: CTA-tile kernel, 1: warp-tile kernel */
     int64_t metadata_bytes;  /* partition + carry scratch held by the plan */
     double algorithmic_bytes;/* compulsory bytes of one SpMV, y = A x */
 } merbit_plan_info;

@@ -53,7 +53,7 @@ class _PlanInfo(C.Structure):
     _fields_ = [
         ("nrow", C.c_int32), ("ncol", C.c_int32), ("nnz", C.c_int32), ("dtype", C.c_int32),
         ("block", C.c_int32), ("items_per_thread", C.c_int32), ("tile_items", C.c_int32),
-        ("num_tiles", C.c_int32), ("vectorized", C.c_int32),
+        ("num_tiles", C.c_int32), ("vectorized", C.c_int32), ("kind", C.c_int32),
         ("metadata_bytes", C.c_int64), ("algorithmic_bytes", C.c_double),
     ]
 
@@ -172,6 +172,7 @@ class PlanInfo:
     tile_items: int
     num_tiles: int
     vectorized: bool
+    kind: int
     metadata_bytes: int
     algorithmic_bytes: float
 
@@ -221,7 +222,7 @@ class Plan:
         i = _PlanInfo()
         _check(lib().merbit_plan_get_info(self._h, C.byref(i)))
         return PlanInfo(i.nrow, i.ncol, i.nnz, i.dtype, i.block, i.items_per_thread,
-                        i.tile_items, i.num_tiles, bool(i.vectorized), i.metadata_bytes,
+                        i.tile_items, i.num_tiles, bool(i.vectorized), i.kind, i.metadata_bytes,
                         i.algorithmic_bytes)
 
     def set_values(self, vals: torch.Tensor) -> None:

@@ -265,6 +265,7 @@ int merbit_plan_get_info(merbit_plan plan, merbit_plan_info* info) {
         meta += (int64_t)(q.num_tiles + 1) * (int64_t)sizeof(int2);
     }
     info->vectorized = plan->vec ? 1 : 0;
+    info->kind = c.kind;
     info->metadata_bytes = meta;
     info->algorithmic_bytes = 4.0 * (plan->nrow + 1.0) +
                               (double)plan->nnz * (4.0 + (double)dtype_size(plan->dtype)) +
