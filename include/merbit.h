@@ -133,6 +133,43 @@ int merbit_plan_config_usable(merbit_plan plan, int32_t idx, int32_t* usable, vo
 int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
                 void* stream);
 
+/* ---------------- k right-hand sides and batches ---------------- */
+
+/* Y[nrow x k] = alpha*A*X[ncol x k] + beta*Y, row-major with leading
+ * dimensions ldx, ldy >= k (elements).  Any k >= 1 (processed in
+ * power-of-two column blocks of at most 32).  The first call for a given
+ * block width allocates that width's carry slots (synchronizes); later
+ * calls allocate nothing and can be captured in a CUDA graph. */
+int merbit_spmm(merbit_plan plan, int32_t k, double alpha, const void* d_x, int64_t ldx,
+                double beta, void* d_y, int64_t ldy, void* stream);
+
+typedef struct merbit_batch_s* merbit_batch;
+
+typedef struct merbit_batch_info {
+    int32_t count, k, dtype;
+    int32_t tile_items;    /* merge items per warp tile */
+    int32_t vector_width;  /* RHS values per lane */
+    int32_t total_tiles;
+    int64_t nnz;
+    double algorithmic_bytes; /* sum over matrices of one SpMM's compulsory bytes */
+} merbit_batch_info;
+
+/* A batch of `count` plans (same dtype) multiplied by k in {1,2,4,8,16,32}
+ * right-hand sides in ONE persistent launch.  The X/Y device buffers of
+ * each matrix are bound at creation (callers refill them between runs);
+ * plans and buffers must outlive the batch.  Synchronizes. */
+int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* plans, int32_t k,
+                        const void* const* d_x, const int64_t* ldx, void* const* d_y,
+                        const int64_t* ldy, void* stream);
+/* Y_i = alpha*A_i*X_i + beta*Y_i for every matrix of the batch: one kernel
+ * launch, no allocation, no synchronization (capturable in a CUDA graph). */
+int merbit_batch_spmm(merbit_batch batch, double alpha, double beta, void* stream);
+/* Times the tile sizes and RHS vector widths the batch can use and keeps the
+ * fastest (the autotuner's choice per batch signature).  Synchronizes. */
+int merbit_batch_tune(merbit_batch batch, void* stream);
+int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info);
+int merbit_batch_destroy(merbit_batch batch);
+
 /* y[nrow] = alpha*A*x + beta*y without allocating any device memory -- for
  * callers that cannot allocate on the call path: code running while a CUDA
  * stream is captured (cudaMalloc cannot be captured), hosts whose device

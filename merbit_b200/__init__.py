@@ -76,6 +76,13 @@ SIGNATURES = {
     "merbit_plan_set_config": (C.c_int, [_P, C.c_int32, _P]),
     "merbit_plan_config_usable": (C.c_int, [_P, C.c_int32, _P, _P]),
     "merbit_plan_check": (C.c_int, [_P, _P]),
+    "merbit_spmm": (C.c_int, [_P, C.c_int32, C.c_double, _P, C.c_int64, C.c_double, _P,
+                              C.c_int64, _P]),
+    "merbit_batch_create": (C.c_int, [_P, C.c_int32, _P, C.c_int32, _P, _P, _P, _P, _P]),
+    "merbit_batch_spmm": (C.c_int, [_P, C.c_double, C.c_double, _P]),
+    "merbit_batch_tune": (C.c_int, [_P, _P]),
+    "merbit_batch_get_info": (C.c_int, [_P, _P]),
+    "merbit_batch_destroy": (C.c_int, [_P]),
     "merbit_spmv_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int,
                                       C.c_double, _P, C.c_double, _P, _P]),
     "merbit_status_string": (C.c_char_p, [C.c_int]),
@@ -250,6 +257,29 @@ class Plan:
                                  _stream_ptr(stream)))
         return y
 
+    def _mat(self, t: torch.Tensor, rows: int, name: str) -> int:
+        if not t.is_cuda or t.dtype != self.xy_dtype:
+            raise TypeError(f"{name} must be a CUDA {self.xy_dtype} tensor")
+        if t.dim() != 2 or t.shape[0] != rows or (rows > 1 and t.stride(1) != 1):
+            raise ValueError(f"{name} must be a row-major ({rows}, k) matrix")
+        return t.stride(0) if rows > 1 else t.shape[1]
+
+    def spmm(self, X: torch.Tensor, Y: torch.Tensor | None = None, alpha: float = 1.0,
+             beta: float = 0.0, stream=None) -> torch.Tensor:
+        """Y = alpha*A*X + beta*Y for row-major X (ncol, k) -> Y (nrow, k)."""
+        ldx = self._mat(X, self.ncol, "X")
+        k = X.shape[1]
+        if Y is None:
+            Y = torch.empty(self.nrow, k, dtype=self.xy_dtype, device=self.device)
+        ldy = self._mat(Y, self.nrow, "Y")
+        if Y.shape[1] != k:
+            raise ValueError("X and Y must have the same number of columns")
+        if k == 0:
+            return Y
+        _check(lib().merbit_spmm(self._h, k, float(alpha), _dptr(X), max(ldx, k), float(beta),
+                                 _dptr(Y), max(ldy, k), _stream_ptr(stream)))
+        return Y
+
     def tune(self, x: torch.Tensor | None = None, stream=None) -> PlanInfo:
         """Time every kernel configuration on this matrix and keep the fastest
         (cached per matrix signature for the process)."""
@@ -277,3 +307,58 @@ class Plan:
     def check(self, stream=None) -> None:
         """Raise MerbitError if a device-side wait of any launch ran out."""
         _check(lib().merbit_plan_check(self._h, _stream_ptr(stream)))
+
+
+class _BatchInfo(C.Structure):
+    _fields_ = [("count", C.c_int32), ("k", C.c_int32), ("dtype", C.c_int32),
+                ("tile_items", C.c_int32), ("vector_width", C.c_int32),
+                ("total_tiles", C.c_int32), ("nnz", C.c_int64), ("algorithmic_bytes", C.c_double)]
+
+
+class Batch:
+    """Many plans times k right-hand sides in one persistent launch
+    (merbit_batch_create / merbit_batch_spmm).  Xs[i] (ncol_i, k) and
+    Ys[i] (nrow_i, k) are bound at creation; refill them between runs."""
+
+    def __init__(self, plans: list[Plan], Xs: list[torch.Tensor], Ys: list[torch.Tensor],
+                 stream=None):
+        if not (len(plans) == len(Xs) == len(Ys)) or not plans:
+            raise ValueError("plans, Xs and Ys must have the same non-zero length")
+        k = Xs[0].shape[1]
+        self.plans, self.Xs, self.Ys, self.k = list(plans), list(Xs), list(Ys), k
+        n = len(plans)
+        hp = (_P * n)(*[p._h for p in plans])
+        hx = (_P * n)(*[_dptr(x) for x in Xs])
+        hy = (_P * n)(*[_dptr(y) for y in Ys])
+        ldx = (C.c_int64 * n)(*[p._mat(x, p.ncol, "X") if x.shape[1] == k else -1
+                                for p, x in zip(plans, Xs)])
+        ldy = (C.c_int64 * n)(*[p._mat(y, p.nrow, "Y") if y.shape[1] == k else -1
+                                for p, y in zip(plans, Ys)])
+        ldx = (C.c_int64 * n)(*[max(v, k) if v >= 0 else -1 for v in ldx])
+        ldy = (C.c_int64 * n)(*[max(v, k) if v >= 0 else -1 for v in ldy])
+        self._h = _P()
+        _check(lib().merbit_batch_create(C.byref(self._h), n, hp, k, hx, ldx, hy, ldy,
+                                         _stream_ptr(stream)))
+
+    def run(self, alpha: float = 1.0, beta: float = 0.0, stream=None) -> None:
+        _check(lib().merbit_batch_spmm(self._h, float(alpha), float(beta), _stream_ptr(stream)))
+
+    def tune(self, stream=None):
+        _check(lib().merbit_batch_tune(self._h, _stream_ptr(stream)))
+        return self.info()
+
+    def info(self) -> dict:
+        i = _BatchInfo()
+        _check(lib().merbit_batch_get_info(self._h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in _BatchInfo._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            lib().merbit_batch_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,305 @@
+// C ABI for the SpMM kernels (spmm.cu): one plan with k right-hand sides,
+// and batches of plans run by one persistent launch.
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "merbit_internal.cuh"
+
+namespace merbit {
+
+int alloc_spmm_slots(SpmmSlots* s, long long nslots, cudaStream_t st) {
+    if (nslots <= 0) nslots = 1;
+    if (nslots > INT_MAX) return fail(MERBIT_ERR_OVERFLOW, "spmm: tiles * k exceeds int32");
+    const size_t words = 4 * (size_t)nslots;
+    MERBIT_CUDA(cudaMalloc(&s->words, sizeof(unsigned long long) * words));
+    MERBIT_CUDA(cudaMalloc(&s->state, sizeof(LaunchState)));
+    MERBIT_CUDA(cudaMemsetAsync(s->words, 0xFF, sizeof(unsigned long long) * words, st));
+    LaunchState init = {};
+    init.epoch = 1u;
+    MERBIT_CUDA(cudaMemcpyAsync(s->state, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    MERBIT_CUDA(cudaStreamSynchronize(st));
+    s->nslots = nslots;
+    return MERBIT_OK;
+}
+
+namespace {
+
+constexpr int kDefaultItems = 256;
+
+bool pow2(int k) { return k > 0 && (k & (k - 1)) == 0; }
+
+// Widest RHS vector per lane (4, 2, 1) that the leading dimension and the
+// pointers allow for k columns of a type of `esz` bytes.
+int pick_vw(int k, long long ldx, const void* x, const void* y, long long ldy, int esz,
+            int items) {
+    for (int vw = 4; vw >= 1; vw >>= 1) {
+        if (vw > k || !spmm_config_exists(k, vw, items)) continue;
+        if (vw == 1) return 1;
+        const size_t a = (size_t)vw * esz;  // vector load size
+        if (ldx % vw != 0) continue;
+        if (((uintptr_t)x % (a < 16 ? a : 16)) != 0) continue;
+        (void)y;
+        (void)ldy;
+        return vw;
+    }
+    return 1;
+}
+
+SpmmDesc make_desc(merbit_plan_s* p, const Partition* part, const void* x, long long ldx, void* y,
+                   long long ldy, int tile_begin) {
+    SpmmDesc d;
+    d.row_ptr = p->row_ptr;
+    d.col = p->col;
+    d.vals = p->vals;
+    d.x = x;
+    d.y = y;
+    d.ldx = ldx;
+    d.ldy = ldy;
+    d.coords = part->coords;
+    d.nrow = p->nrow;
+    d.nnz = p->nnz;
+    d.num_tiles = part->num_tiles;
+    d.tile_begin = tile_begin;
+    return d;
+}
+
+// One launch over columns [0, kk) of X / Y (pointers already offset).
+int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long ldx, double beta,
+               void* y, long long ldy, cudaStream_t s) {
+    const int items = kDefaultItems;
+    const Partition* part = nullptr;
+    int st = plan_partition(p, items, &part, s);
+    if (st != MERBIT_OK) return st;
+    const long long key = ((long long)kk << 20) | items;
+    auto it = p->spmm_slots.find(key);
+    if (it == p->spmm_slots.end()) {
+        SpmmSlots sl;
+        st = alloc_spmm_slots(&sl, (long long)part->num_tiles * kk, s);
+        if (st != MERBIT_OK) return st;
+        it = p->spmm_slots.emplace(key, sl).first;
+    }
+    const int esz = (int)xy_size(p->dtype);
+    const int vw = pick_vw(kk, ldx, x, y, ldy, esz, items);
+    SpmmLaunch a = {};
+    a.single = make_desc(p, part, x, ldx, y, ldy, 0);
+    a.descs = nullptr;
+    a.ndesc = 0;
+    a.nslots = (int)it->second.nslots;
+    a.slots = it->second.words;
+    a.xch = it->second.words + 2 * (size_t)it->second.nslots;
+    a.state = it->second.state;
+    a.total_tiles = part->num_tiles;
+    a.alpha = alpha;
+    a.beta = beta;
+    return spmm_launch(p->dtype, kk, vw, items, a, s);
+}
+
+}  // namespace
+}  // namespace merbit
+
+// Batch of plans sharing one persistent launch.
+struct merbit_batch_s {
+    int count = 0, k = 0, dtype = 0, items = 256, vw = 1;
+    std::vector<merbit_plan_s*> plans;
+    std::vector<const void*> x;
+    std::vector<void*> y;
+    std::vector<long long> ldx, ldy;
+    merbit::SpmmDesc* d_descs = nullptr;
+    int total_tiles = 0;
+    merbit::SpmmSlots slots;
+    double algorithmic_bytes = 0.0;
+    long long nnz = 0;
+};
+
+using namespace merbit;
+
+namespace {
+
+int batch_build(merbit_batch_s* b, int items, cudaStream_t s) {
+    std::vector<SpmmDesc> h(b->count);
+    long long tot = 0;
+    for (int i = 0; i < b->count; ++i) {
+        const Partition* part = nullptr;
+        int st = plan_partition(b->plans[i], items, &part, s);
+        if (st != MERBIT_OK) return st;
+        if (tot + part->num_tiles > INT_MAX) return fail(MERBIT_ERR_OVERFLOW, "batch: too many tiles");
+        h[i] = make_desc(b->plans[i], part, b->x[i], b->ldx[i], b->y[i], b->ldy[i], (int)tot);
+        tot += part->num_tiles;
+    }
+    int vw = 4;
+    const int esz = (int)xy_size(b->dtype);
+    for (int i = 0; i < b->count; ++i)
+        vw = std::min(vw, pick_vw(b->k, b->ldx[i], b->x[i], b->y[i], b->ldy[i], esz, items));
+    if (!spmm_config_exists(b->k, vw, items)) vw = 1;
+    if (b->d_descs == nullptr) MERBIT_CUDA(cudaMalloc(&b->d_descs, sizeof(SpmmDesc) * b->count));
+    MERBIT_CUDA(cudaMemcpyAsync(b->d_descs, h.data(), sizeof(SpmmDesc) * b->count,
+                                cudaMemcpyHostToDevice, s));
+    if (b->slots.nslots < tot * b->k) {
+        cudaFree(b->slots.words);
+        cudaFree(b->slots.state);
+        b->slots = SpmmSlots();
+        int st = alloc_spmm_slots(&b->slots, tot * b->k, s);
+        if (st != MERBIT_OK) return st;
+    }
+    MERBIT_CUDA(cudaStreamSynchronize(s));
+    b->items = items;
+    b->vw = vw;
+    b->total_tiles = (int)tot;
+    return MERBIT_OK;
+}
+
+int batch_run(merbit_batch_s* b, double alpha, double beta, cudaStream_t s) {
+    SpmmLaunch a = {};
+    a.descs = b->d_descs;
+    a.ndesc = b->count;
+    a.nslots = (int)b->slots.nslots;
+    a.slots = b->slots.words;
+    a.xch = b->slots.words + 2 * (size_t)b->slots.nslots;
+    a.state = b->slots.state;
+    a.total_tiles = b->total_tiles;
+    a.alpha = alpha;
+    a.beta = beta;
+    return spmm_launch(b->dtype, b->k, b->vw, b->items, a, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int merbit_spmm(merbit_plan plan, int32_t k, double alpha, const void* d_x, int64_t ldx,
+                double beta, void* d_y, int64_t ldy, void* stream) {
+    if (!plan) return fail(MERBIT_ERR_INVALID, "spmm: plan is null");
+    if (k < 1) return fail(MERBIT_ERR_INVALID, "spmm: k < 1");
+    if (ldx < k || ldy < k) return fail(MERBIT_ERR_INVALID, "spmm: leading dimension < k");
+    if (plan->nrow == 0) return MERBIT_OK;
+    if (!d_y || (plan->ncol > 0 && !d_x)) return fail(MERBIT_ERR_INVALID, "spmm: X/Y is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t esz = xy_size(plan->dtype);
+    // power-of-two column blocks of at most 32
+    int j = 0;
+    while (j < k) {
+        int kk = 32;
+        while (kk > k - j) kk >>= 1;
+        const char* xb = static_cast<const char*>(d_x) + (size_t)j * esz;
+        char* yb = static_cast<char*>(d_y) + (size_t)j * esz;
+        int st = spmm_block(plan, kk, alpha, xb, ldx, beta, yb, ldy, s);
+        if (st != MERBIT_OK) return st;
+        j += kk;
+    }
+    return MERBIT_OK;
+}
+
+int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* plans, int32_t k,
+                        const void* const* d_x, const int64_t* ldx, void* const* d_y,
+                        const int64_t* ldy, void* stream) {
+    if (!batch) return fail(MERBIT_ERR_INVALID, "batch_create: batch is null");
+    *batch = nullptr;
+    if (count < 1 || !plans || !d_x || !d_y || !ldx || !ldy)
+        return fail(MERBIT_ERR_INVALID, "batch_create: bad arguments");
+    if (!pow2(k) || k > 32) return fail(MERBIT_ERR_UNSUPPORTED, "batch_create: k must be 1, 2, 4, 8, 16 or 32");
+    auto* b = new merbit_batch_s();
+    b->count = count;
+    b->k = k;
+    b->dtype = plans[0] ? plans[0]->dtype : 0;
+    for (int i = 0; i < count; ++i) {
+        merbit_plan_s* p = plans[i];
+        if (!p || p->dtype != b->dtype || ldx[i] < k || ldy[i] < k ||
+            (p->nrow > 0 && !d_y[i]) || (p->ncol > 0 && !d_x[i])) {
+            delete b;
+            return fail(MERBIT_ERR_INVALID, "batch_create: plan " + std::to_string(i) +
+                                                " is null, of another dtype, or has bad X/Y");
+        }
+        b->plans.push_back(p);
+        b->x.push_back(d_x[i]);
+        b->y.push_back(d_y[i]);
+        b->ldx.push_back(ldx[i]);
+        b->ldy.push_back(ldy[i]);
+        b->nnz += p->nnz;
+        b->algorithmic_bytes += 4.0 * (p->nrow + 1.0) + (double)p->nnz * (4.0 + (double)dtype_size(p->dtype)) +
+                                (double)k * (double)xy_size(p->dtype) * ((double)p->ncol + p->nrow);
+    }
+    int st = batch_build(b, kDefaultItems, (cudaStream_t)stream);
+    if (st != MERBIT_OK) {
+        merbit_batch_destroy(b);
+        return st;
+    }
+    *batch = b;
+    return MERBIT_OK;
+}
+
+int merbit_batch_spmm(merbit_batch batch, double alpha, double beta, void* stream) {
+    if (!batch) return fail(MERBIT_ERR_INVALID, "batch_spmm: batch is null");
+    return batch_run(batch, alpha, beta, (cudaStream_t)stream);
+}
+
+int merbit_batch_tune(merbit_batch batch, void* stream) {
+    if (!batch) return fail(MERBIT_ERR_INVALID, "batch_tune: batch is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    // candidates: tile items x widest legal vector width (narrower widths too)
+    const int items_c[2] = {256, 512};
+    int best_items = batch->items, best_vw = batch->vw;
+    float best = 1e30f;
+    cudaEvent_t e0, e1;
+    MERBIT_CUDA(cudaEventCreate(&e0));
+    MERBIT_CUDA(cudaEventCreate(&e1));
+    int st = MERBIT_OK;
+    for (int ii = 0; ii < 2 && st == MERBIT_OK; ++ii) {
+        st = batch_build(batch, items_c[ii], s);
+        if (st != MERBIT_OK) break;
+        const int vmax = batch->vw;
+        for (int vw = vmax; vw >= 1 && st == MERBIT_OK; vw >>= 1) {
+            if (!spmm_config_exists(batch->k, vw, items_c[ii])) continue;
+            batch->vw = vw;
+            for (int w = 0; w < 2 && st == MERBIT_OK; ++w) st = batch_run(batch, 1.0, 0.0, s);
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < 3 && st == MERBIT_OK; ++r) st = batch_run(batch, 1.0, 0.0, s);
+            cudaEventRecord(e1, s);
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                st = cuda_fail(cudaGetLastError(), "batch_tune");
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                best_items = items_c[ii];
+                best_vw = vw;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != MERBIT_OK) return st;
+    st = batch_build(batch, best_items, s);
+    if (st != MERBIT_OK) return st;
+    batch->vw = best_vw;
+    return MERBIT_OK;
+}
+
+int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info) {
+    if (!batch || !info) return fail(MERBIT_ERR_INVALID, "batch_get_info: null pointer");
+    info->count = batch->count;
+    info->k = batch->k;
+    info->dtype = batch->dtype;
+    info->tile_items = batch->items;
+    info->vector_width = batch->vw;
+    info->total_tiles = batch->total_tiles;
+    info->nnz = batch->nnz;
+    info->algorithmic_bytes = batch->algorithmic_bytes;
+    return MERBIT_OK;
+}
+
+int merbit_batch_destroy(merbit_batch batch) {
+    if (!batch) return MERBIT_OK;
+    cudaFree(batch->d_descs);
+    cudaFree(batch->slots.words);
+    cudaFree(batch->slots.state);
+    delete batch;
+    return MERBIT_OK;
+}
+
+}  // extern "C"

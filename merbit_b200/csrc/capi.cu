@@ -35,8 +35,8 @@ int validate_csr(const int32_t* row_ptr, const int32_t* col, int nrow, int ncol,
                  cudaStream_t s);
 
 namespace {
-
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+}  // namespace
 
 // Ensures the plan holds a partition for `tile_items` and enough carry
 // slots; returns it in *out.
@@ -64,6 +64,8 @@ int plan_partition(merbit_plan_s* p, int tile_items, const Partition** out, cuda
     *out = &p->parts.back();
     return MERBIT_OK;
 }
+
+namespace {
 
 // Whether configuration idx can run this plan (builds its partition).
 int plan_config_ok(merbit_plan_s* p, int idx, bool* ok, cudaStream_t s) {
@@ -242,6 +244,10 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
 int merbit_plan_destroy(merbit_plan plan) {
     if (!plan) return MERBIT_OK;
     for (auto& q : plan->parts) cudaFree(q.coords);
+    for (auto& kv : plan->spmm_slots) {
+        cudaFree(kv.second.words);
+        cudaFree(kv.second.state);
+    }
     cudaFree(plan->carry);
     cudaFree(plan->state);
     delete plan;

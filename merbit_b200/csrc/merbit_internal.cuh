@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <climits>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -333,6 +334,15 @@ constexpr int warp_rp_cap(int ipt) { return (32 * ipt) / 3 + 16; }
 int build_partition(const int32_t* row_ptr, int nrow, int nnz, int tile_items, Partition* out,
                     cudaStream_t s);
 
+// Carry / swap words of one SpMM slot family (2 parities x 2 arrays x
+// tiles x k) with its own launch state.
+struct SpmmSlots {
+    unsigned long long* words = nullptr;
+    LaunchState* state = nullptr;
+    long long nslots = 0;  // tiles * k
+};
+int alloc_spmm_slots(SpmmSlots* s, long long nslots, cudaStream_t st);
+
 // SpMV kernel configurations (spmv.cu).
 struct SpmvConfig {
     int kind;  // 0: CTA-tile kernel, 1: warp-tile kernel
@@ -363,6 +373,37 @@ struct SpmvLaunch {
 };
 int spmv_launch(int dtype, int cfg, bool vec, const SpmvLaunch& a, cudaStream_t s);
 
+// One matrix of an SpMM launch (spmm.cu).  Tiles of ITEMS merge items;
+// coords are the matrix's own partition (local tile indices), tile_begin
+// its first tile in the launch's tile index space.
+struct SpmmDesc {
+    const int32_t* row_ptr;
+    const int32_t* col;
+    const void* vals;
+    const void* x;
+    void* y;
+    long long ldx, ldy;
+    const int2* coords;
+    int nrow, nnz, num_tiles, tile_begin;
+};
+
+struct SpmmLaunch {
+    SpmmDesc single;        // used when ndesc == 0
+    const SpmmDesc* descs;  // device array of ndesc descriptors (a batch)
+    int ndesc;
+    unsigned long long* slots;  // 2 * nslots carry words (nslots = total_tiles * k)
+    unsigned long long* xch;    // 2 * nslots boundary-swap words
+    int nslots;
+    LaunchState* state;
+    int total_tiles;
+    double alpha, beta;
+};
+
+// Launches the SpMM kernel for k right-hand sides, vw values per lane and
+// `items` merge items per warp tile.
+int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s);
+bool spmm_config_exists(int k, int vw, int items);
+
 }  // namespace merbit
 
 // Host-side plan object.
@@ -380,4 +421,10 @@ struct merbit_plan_s {
     unsigned long long* carry = nullptr;
     int slots = 0;
     merbit::LaunchState* state = nullptr;
+    // SpMM carry slots, keyed by (k << 20 | tile items)
+    std::map<long long, merbit::SpmmSlots> spmm_slots;
 };
+
+namespace merbit {
+int plan_partition(merbit_plan_s* p, int tile_items, const Partition** out, cudaStream_t s);
+}

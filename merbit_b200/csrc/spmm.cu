@@ -1,0 +1,505 @@
+// Merge-path SpMM for sm_100a:  Y = alpha * A X + beta * Y  with K
+// right-hand sides (row-major X [ncol x ldx], Y [nrow x ldy]), for one
+// matrix or a batch of matrices in one persistent launch.
+//
+// The merge path of each matrix is cut into warp tiles of ITEMS merge
+// items, as for the SpMV (spmv_warp.cu): lane 0 stages the tile's row_ptr
+// window, col_idx slice and vals slice with cp.async.bulk on an mbarrier.
+// Inside the warp, lanes form groups of K/VW lanes (VW = RHS values per
+// lane: 1, 2 or 4); each group walks its own segment of ITEMS/G merge items
+// (G groups per warp), lane j of a group owning RHS columns
+// [j*VW, j*VW + VW).  The x rows of the next CH nonzeros are gathered while
+// the current CH are accumulated, so gathers overlap the walk.  A rows that
+// ends inside a segment is written directly (coalesced across the group's
+// lanes); the group segmented scan (shuffles with stride K/VW) finishes the
+// rows split between groups, and rows split between tiles are finished
+// per RHS column exactly as in the SpMV: two-tile rows by an atomicExch
+// swap of the partials (the later side writes carry + head), longer rows by
+// a fixed-order look-back over published per-tile partials.  No float
+// atomics: results are bitwise reproducible.
+//
+// Batches: the tiles of all matrices form one index space; matrix m owns
+// tiles [tile_begin_m, tile_begin_m + num_tiles_m).  Warps of the
+// persistent cooperative grid take tiles round-robin, so one launch covers
+// the whole batch, and the launch can be captured in a CUDA graph and
+// replayed (carry slots are per launch parity, as in the SpMV).
+#include <type_traits>
+
+#include "merbit_internal.cuh"
+
+namespace merbit {
+
+namespace {
+
+constexpr size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+template <int VW>
+__device__ __forceinline__ void ld_vec(const float* p, float (&o)[VW]) {
+    if (VW == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+        o[2] = t.z;
+        o[3] = t.w;
+    } else if (VW == 2) {
+        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+    } else {
+        o[0] = __ldg(p);
+    }
+}
+template <int VW>
+__device__ __forceinline__ void ld_vec(const double* p, double (&o)[VW]) {
+    if (VW >= 2) {
+#pragma unroll
+        for (int q = 0; q < VW; q += 2) {
+            const double2 t = __ldg(reinterpret_cast<const double2*>(p) + q / 2);
+            o[q] = t.x;
+            o[q + 1] = t.y;
+        }
+    } else {
+        o[0] = __ldg(p);
+    }
+}
+
+template <typename Y>
+__device__ __forceinline__ void st_row(Y* __restrict__ y, size_t off, double v, double alpha,
+                                       double beta) {
+    double o = alpha * v;
+    if (beta != 0.0) o += beta * (double)y[off];
+    y[off] = (Y)o;
+}
+
+__device__ __forceinline__ unsigned long long dbits(double v) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return b == kEmpty ? 0x7FF8000000000000ull : b;
+}
+
+}  // namespace
+
+template <int DT, int K, int VW, int ITEMS>
+struct SpmmTile {
+    using Pr = Prec<DT>;
+    using V = typename Pr::V;
+    using X = typename Pr::X;
+    using Y = typename Pr::Y;
+    using P = typename Pr::P;
+    using Acc = typename Pr::Acc;
+    static constexpr int LPG = K / VW;      // lanes per group
+    static constexpr int G = 32 / LPG;      // groups per warp
+    static constexpr int SEG = ITEMS / G;   // merge items per group
+    static constexpr int CH = 8 / VW;       // nonzeros gathered ahead (8 values per lane)
+    static constexpr int CAP = ITEMS + 32;
+    static constexpr int RPC = ITEMS + 16;  // row_ptr window (any rows per tile)
+    static constexpr size_t rp_bytes = a16((size_t)RPC * 4);
+    static constexpr size_t col_bytes = a16((size_t)CAP * 4);
+    static constexpr size_t val_bytes = a16((size_t)CAP * sizeof(V));
+    static constexpr size_t bar_offset = rp_bytes + col_bytes + val_bytes;
+    static constexpr size_t bytes = bar_offset + 16;
+    static constexpr int GV = 16 / (int)sizeof(V);
+    static_assert(LPG >= 1 && LPG <= 32 && 32 % LPG == 0, "K/VW must divide 32");
+    static_assert(SEG * G == ITEMS, "ITEMS must be a multiple of the group count");
+
+    static __device__ __forceinline__ void issue(const SpmmDesc& d, int lt, unsigned char* ws,
+                                                 uint64_t* bar, int lane) {
+        const int2 c0 = d.coords[lt];
+        const int2 c1 = d.coords[lt + 1];
+        int* s_rp = reinterpret_cast<int*>(ws);
+        int* s_col = reinterpret_cast<int*>(ws + rp_bytes);
+        V* s_val = reinterpret_cast<V*>(ws + rp_bytes + col_bytes);
+        const V* vals = static_cast<const V*>(d.vals);
+        const int nrp = d.nrow + 1;
+        auto bb = [](int s, int e, int n, int g, int esz) -> unsigned {
+            if (e <= s) return 0u;
+            const int base = s & ~(g - 1), lim = n & ~(g - 1);
+            const int b_end = min((e + g - 1) & ~(g - 1), lim);
+            return b_end > base ? (unsigned)(b_end - base) * (unsigned)esz : 0u;
+        };
+        const unsigned tot = bb(c0.y, c1.y + 1, nrp, 4, 4) + bb(c0.x, c1.x, d.nnz, 4, 4) +
+                             bb(c0.x, c1.x, d.nnz, GV, (int)sizeof(V));
+        __syncwarp();
+        if (lane == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive_expect_tx(bar, tot);
+        }
+        const uint64_t pol = l2_evict_first_policy();
+        auto stage = [&](auto* dst, const auto* src, int s, int e, int n) {
+            using T = typename std::remove_pointer<decltype(dst)>::type;
+            constexpr int GG = 16 / (int)sizeof(T);
+            if (e <= s) return;
+            const int base = s & ~(GG - 1), lim = n & ~(GG - 1);
+            const int b_end = min((e + GG - 1) & ~(GG - 1), lim);
+            if (b_end > base && lane == 0)
+                bulk_g2s(dst, src + base, (unsigned)(b_end - base) * (unsigned)sizeof(T), bar, pol);
+            const int p0 = max(b_end, s);
+            if (lane < e - p0) dst[p0 + lane - base] = src[p0 + lane];
+        };
+        stage(s_rp, d.row_ptr, c0.y, c1.y + 1, nrp);
+        stage(s_col, d.col, c0.x, c1.x, d.nnz);
+        stage(s_val, vals, c0.x, c1.x, d.nnz);
+    }
+
+    // Row ends of the tile as nonzero positions relative to x0.
+    static __device__ __forceinline__ int row_end(const int* s_rp, int rpo, int r, int x0) {
+        return s_rp[rpo + r + 1] - x0;
+    }
+
+    static __device__ __forceinline__ void process(const SpmmLaunch& a, const SpmmDesc& d,
+                                                   int u, int lt, unsigned epoch,
+                                                   unsigned char* ws, int lane) {
+        unsigned long long* slots = a.slots;
+        unsigned long long* xch = a.xch;
+        const int nslots = a.nslots;
+        LaunchState* st = a.state;
+        const int* s_rp = reinterpret_cast<const int*>(ws);
+        const int* s_col = reinterpret_cast<const int*>(ws + rp_bytes);
+        const V* s_val = reinterpret_cast<const V*>(ws + rp_bytes + col_bytes);
+        const int2 c0 = d.coords[lt];
+        const int2 c1 = d.coords[lt + 1];
+        const int prev_x = lt > 0 ? d.coords[lt - 1].x : 0;
+        const int x0 = c0.x, y0 = c0.y, x1 = c1.x, y1 = c1.y;
+        const int nz = x1 - x0, nr = y1 - y0, L = nz + nr;
+        const int rpo = y0 - (y0 & ~3);
+        const int col_o = x0 - (x0 & ~3);
+        const int val_o = x0 - (x0 & ~(GV - 1));
+        const int g = lane / LPG;        // group
+        const int jl = lane % LPG;       // lane within group
+        const int j0 = jl * VW;          // first RHS column of this lane
+        const X* __restrict__ xm = static_cast<const X*>(d.x);
+        Y* __restrict__ ym = static_cast<Y*>(d.y);
+        const double alpha = a.alpha, beta = a.beta;
+
+        // ---- this group's segment [ds, de) of the tile's merge path
+        const int ds = min(g * SEG, L), de = min(ds + SEG, L);
+        auto search = [&](int dl, int& lx, int& ly) {
+            int lo = max(dl - nz, 0), hi = min(dl, nr);
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (s_rp[rpo + mid + 1] - x0 <= dl - mid - 1)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            ly = lo;
+            lx = dl - lo;
+        };
+        int lx, ly, lx_end, ly_end;
+        search(ds, lx, ly);
+        search(de, lx_end, ly_end);
+
+        Acc acc[VW];
+#pragma unroll
+        for (int v = 0; v < VW; ++v) acc[v].zero();
+        int first_row = -1;
+        double first_val[VW];
+#pragma unroll
+        for (int v = 0; v < VW; ++v) first_val[v] = 0.0;
+        auto emit = [&](int r) {
+            if (first_row < 0) {
+                first_row = r;
+#pragma unroll
+                for (int v = 0; v < VW; ++v) first_val[v] = acc[v].value();
+            } else {
+#pragma unroll
+                for (int v = 0; v < VW; ++v)
+                    st_row(ym, (size_t)(y0 + r) * d.ldy + j0 + v, acc[v].value(), alpha, beta);
+            }
+#pragma unroll
+            for (int v = 0; v < VW; ++v) acc[v].zero();
+        };
+
+        // ---- walk: chunks of CH nonzeros, the next chunk's x rows in flight
+        // (two named buffers, so both stay in registers)
+        X xa[CH][VW], xb[CH][VW];
+        V va[CH], vb[CH];
+        auto load_chunk = [&](int c, X (&xr)[CH][VW], V (&vv)[CH]) {
+#pragma unroll
+            for (int t = 0; t < CH; ++t) {
+                if (c + t < lx_end) {
+                    const int e = c + t;
+                    const int colv = s_col[col_o + e];
+                    vv[t] = s_val[val_o + e];
+                    ld_vec<VW>(xm + (size_t)colv * d.ldx + j0, xr[t]);
+                }
+            }
+        };
+        auto consume = [&](int c, const X (&xr)[CH][VW], const V (&vv)[CH]) {
+#pragma unroll
+            for (int t = 0; t < CH; ++t) {
+                const int e = c + t;
+                if (e < lx_end) {
+                    while (ly < ly_end && row_end(s_rp, rpo, ly, x0) <= e) {
+                        emit(ly);
+                        ++ly;
+                    }
+                    const P av = to_p(vv[t]);
+#pragma unroll
+                    for (int v = 0; v < VW; ++v) acc[v].add(av * (P)xr[t][v]);
+                }
+            }
+        };
+        if (lx < lx_end) load_chunk(lx, xa, va);
+        for (int c = lx; c < lx_end; c += 2 * CH) {
+            if (c + CH < lx_end) load_chunk(c + CH, xb, vb);
+            consume(c, xa, va);
+            if (c + CH >= lx_end) break;
+            if (c + 2 * CH < lx_end) load_chunk(c + 2 * CH, xa, va);
+            consume(c + CH, xb, vb);
+        }
+        while (ly < ly_end) {
+            emit(ly);
+            ++ly;
+        }
+
+        // ---- group segmented scan, per RHS column (stride LPG lanes)
+        int f = first_row >= 0;
+        double sv[VW];
+#pragma unroll
+        for (int v = 0; v < VW; ++v) sv[v] = acc[v].value();
+#pragma unroll
+        for (int o = 1; o < G; o <<= 1) {
+            double t[VW];
+#pragma unroll
+            for (int v = 0; v < VW; ++v) t[v] = __shfl_up_sync(0xFFFFFFFFu, sv[v], o * LPG);
+            const int tf = __shfl_up_sync(0xFFFFFFFFu, f, o * LPG);
+            if (g >= o) {
+                if (!f) {
+#pragma unroll
+                    for (int v = 0; v < VW; ++v) sv[v] = t[v] + sv[v];
+                }
+                f |= tf;
+            }
+        }
+        double ev[VW];
+#pragma unroll
+        for (int v = 0; v < VW; ++v) {
+            ev[v] = G > 1 ? __shfl_up_sync(0xFFFFFFFFu, sv[v], LPG) : 0.0;
+            if (g == 0) ev[v] = 0.0;
+        }
+        const int rs = s_rp[rpo];
+        const bool need_lb = nr > 0 && rs < x0;
+        const bool holds_first = first_row == 0 && need_lb;
+        double rv[VW];
+#pragma unroll
+        for (int v = 0; v < VW; ++v) rv[v] = ev[v] + first_val[v];
+        if (first_row >= 0 && !holds_first) {
+#pragma unroll
+            for (int v = 0; v < VW; ++v)
+                st_row(ym, (size_t)(y0 + first_row) * d.ldy + j0 + v, rv[v], alpha, beta);
+        }
+
+        // ---- the tile's trailing partial (last group): published, and
+        // swapped with the next tile when the row began in this tile
+        const size_t par = (size_t)(epoch & 1u) * nslots;
+        if (g == G - 1) {
+#pragma unroll
+            for (int v = 0; v < VW; ++v)
+                st_relaxed_u64(slots + par + (size_t)u * K + j0 + v, dbits(sv[v]));
+            if (y1 < d.nrow && lt + 1 < d.num_tiles) {
+                const int rs1 = s_rp[rpo + nr];
+                if (rs1 >= x0 && rs1 < x1) {
+#pragma unroll
+                    for (int v = 0; v < VW; ++v) {
+                        const unsigned long long o =
+                            atomicExch(xch + par + (size_t)(u + 1) * K + j0 + v, dbits(sv[v]));
+                        if (o != kEmpty)
+                            st_row(ym, (size_t)y1 * d.ldy + j0 + v,
+                                   sv[v] + __longlong_as_double((long long)o), alpha, beta);
+                    }
+                }
+            }
+        }
+
+        // ---- row y0 when it began in an earlier tile
+        if (need_lb) {
+            if (prev_x <= rs) {
+                if (holds_first) {
+#pragma unroll
+                    for (int v = 0; v < VW; ++v) {
+                        const unsigned long long o =
+                            atomicExch(xch + par + (size_t)u * K + j0 + v, dbits(rv[v]));
+                        if (o != kEmpty)
+                            st_row(ym, (size_t)y0 * d.ldy + j0 + v,
+                                   __longlong_as_double((long long)o) + rv[v], alpha, beta);
+                    }
+                }
+            } else {
+                // fixed-order look-back: steps of 32/K tiles x K columns
+                // (K <= 32), lane l reading column l % K of tile base - l / K
+                constexpr int TPS = 32 / K > 0 ? 32 / K : 1;
+                double tot = 0.0;  // column (lane % K) of the sum
+                int base = lt - 1;
+                for (;;) {
+                    const int tq = base - lane / K;
+                    const bool lane_valid = lane < TPS * K;
+                    const bool valid = lane_valid && tq >= 0;
+                    const int cx = valid ? d.coords[tq].x : 0;
+                    const unsigned m = __ballot_sync(0xFFFFFFFFu, lane_valid && (tq < 0 || cx <= rs));
+                    // first tile (lowest lane/K) that holds the row start
+                    const int last_t = m ? (__ffs(m) - 1) / K : TPS - 1;
+                    double c = 0.0;
+                    if (valid && lane / K <= last_t) {
+                        const unsigned long long* p =
+                            slots + par + (size_t)(d.tile_begin + tq) * K + (lane % K);
+                        unsigned long long bits = ld_relaxed_u64(p);
+                        if (bits == kEmpty) {
+                            const unsigned long long t0 = global_timer_ns();
+                            while ((bits = ld_relaxed_u64(p)) == kEmpty) {
+                                __nanosleep(32);
+                                if (*(volatile int*)&st->error != 0) break;
+                                if (global_timer_ns() - t0 > kCarryWaitNs) {
+                                    atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
+                                    break;
+                                }
+                            }
+                        }
+                        c = bits == kEmpty ? 0.0 : __longlong_as_double((long long)bits);
+                    }
+                    // sum over the step's tiles, per column (lanes l, l+K, ...)
+#pragma unroll
+                    for (int o = K; o < 32; o <<= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+                    tot += c;
+                    if (m) break;
+                    base -= TPS;
+                }
+                double tv[VW];
+#pragma unroll
+                for (int v = 0; v < VW; ++v) tv[v] = __shfl_sync(0xFFFFFFFFu, tot, j0 + v);
+                if (holds_first) {
+#pragma unroll
+                    for (int v = 0; v < VW; ++v)
+                        st_row(ym, (size_t)y0 * d.ldy + j0 + v, tv[v] + rv[v], alpha, beta);
+                }
+            }
+        }
+    }
+};
+
+template <int DT, int K, int VW, int ITEMS, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) spmm_kernel(const SpmmLaunch a) {
+    using T = SpmmTile<DT, K, VW, ITEMS>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ unsigned s_epoch;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_epoch = *(volatile unsigned*)&a.state->epoch;
+    unsigned char* ws = smem + (size_t)warp * T::bytes;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ws + T::bar_offset);
+    if (lane == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const unsigned epoch = s_epoch;
+    reset_other_parity(a.slots, a.nslots, epoch);
+    reset_other_parity(a.xch, a.nslots, epoch);
+    const int nw = (int)gridDim.x * WARPS;
+    unsigned phase = 0;
+    int m = 0;  // matrix of the current tile (tiles are visited in increasing order)
+    for (int u = (int)blockIdx.x * WARPS + warp; u < a.total_tiles; u += nw) {
+        const SpmmDesc* dp;
+        if (a.ndesc == 0) {
+            dp = &a.single;
+        } else {
+            while (m + 1 < a.ndesc && a.descs[m + 1].tile_begin <= u) ++m;
+            dp = a.descs + m;
+        }
+        const SpmmDesc& d = *dp;
+        const int lt = u - d.tile_begin;
+        T::issue(d, lt, ws, bar, lane);
+        const bool ok = __all_sync(0xFFFFFFFFu, mbar_wait_bounded(bar, phase, a.state));
+        phase ^= 1u;
+        __syncwarp();
+        if (ok) T::process(a, d, u, lt, epoch, ws, lane);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) finish_launch(a.state, epoch);
+}
+
+namespace {
+
+template <int DT, int K, int VW, int ITEMS, int WARPS>
+int launch_spmm_cfg(const SpmmLaunch& a, cudaStream_t s) {
+    using T = SpmmTile<DT, K, VW, ITEMS>;
+    constexpr size_t smem = T::bytes * WARPS;
+    static int grid_cap[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmm: device ordinal >= 64");
+    auto kern = spmm_kernel<DT, K, VW, ITEMS, WARPS>;
+    if (grid_cap[dev] == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(spmm)");
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem);
+        if (e != cudaSuccess) return cuda_fail(e, "occupancy(spmm)");
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        grid_cap[dev] = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
+    }
+    const long long need = ((long long)a.total_tiles + WARPS - 1) / WARPS;
+    const int grid = (int)(need < grid_cap[dev] ? need : grid_cap[dev]);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(WARPS * 32);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e == cudaSuccess ? (int)MERBIT_OK : cuda_fail(e, "spmm_kernel launch");
+}
+
+// Configurations: (K, VW, ITEMS).  WARPS = 4.
+template <int DT>
+int launch_spmm_dt(int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s) {
+#define MERBIT_SPMM_CASE(KK, VV, II) \
+    if (k == KK && vw == VV && items == II) return launch_spmm_cfg<DT, KK, VV, II, 4>(a, s);
+    MERBIT_SPMM_CASE(1, 1, 256)
+    MERBIT_SPMM_CASE(2, 1, 256)
+    MERBIT_SPMM_CASE(2, 2, 256)
+    MERBIT_SPMM_CASE(4, 1, 256)
+    MERBIT_SPMM_CASE(4, 2, 256)
+    MERBIT_SPMM_CASE(4, 4, 256)
+    MERBIT_SPMM_CASE(8, 1, 256)
+    MERBIT_SPMM_CASE(8, 2, 256)
+    MERBIT_SPMM_CASE(8, 4, 256)
+    MERBIT_SPMM_CASE(16, 1, 256)
+    MERBIT_SPMM_CASE(16, 2, 256)
+    MERBIT_SPMM_CASE(16, 4, 256)
+    MERBIT_SPMM_CASE(32, 1, 256)
+    MERBIT_SPMM_CASE(32, 2, 256)
+    MERBIT_SPMM_CASE(32, 4, 256)
+    MERBIT_SPMM_CASE(1, 1, 512)
+    MERBIT_SPMM_CASE(4, 4, 512)
+    MERBIT_SPMM_CASE(8, 4, 512)
+    MERBIT_SPMM_CASE(16, 4, 512)
+    MERBIT_SPMM_CASE(32, 4, 512)
+#undef MERBIT_SPMM_CASE
+    return fail(MERBIT_ERR_INVALID, "spmm: no such configuration");
+}
+
+}  // namespace
+
+bool spmm_config_exists(int k, int vw, int items) {
+    if (items == 256) return (k == 1 && vw == 1) || (k >= 2 && k <= 32 && (k & (k - 1)) == 0 && vw <= 4 && vw <= k && (vw & (vw - 1)) == 0 && !(k == 2 && vw == 4));
+    if (items == 512) return (k == 1 && vw == 1) || (k >= 4 && k <= 32 && (k & (k - 1)) == 0 && vw == 4);
+    return false;
+}
+
+int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s) {
+    if (a.total_tiles <= 0) return MERBIT_OK;
+    switch (dtype) {
+    case MERBIT_F64: return launch_spmm_dt<MERBIT_F64>(k, vw, items, a, s);
+    case MERBIT_F32: return launch_spmm_dt<MERBIT_F32>(k, vw, items, a, s);
+    case MERBIT_BF16: return launch_spmm_dt<MERBIT_BF16>(k, vw, items, a, s);
+    }
+    return fail(MERBIT_ERR_INVALID, "spmm: bad dtype");
+}
+
+}  // namespace merbit

@@ -184,6 +184,46 @@ struct WarpTile {
         const int x0 = c0.x, y0 = c0.y, x1 = c1.x, y1 = c1.y;
         const int nz = x1 - x0, nr = y1 - y0, L = nz + nr;
         const int rp_base = y0 & ~3, col_base = x0 & ~3, val_base = x0 & ~(GV - 1);
+        const int rpo0 = y0 - rp_base;  // staged index of row_ptr[y0]
+
+        // ---- tile inside one row (no row ends: the common case for long rows
+        // of power-law matrices, the reference's fast_track,
+        // include/tile.cuh:267-290): the tile's partial is just the sum of
+        // its products -- lane sums in a fixed order, then a butterfly.
+        if (nr == 0) {
+            const X* __restrict__ xv = static_cast<const X*>(a.x);
+            X xg[IPT];
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                const int i = lane + 32 * j;
+                xg[j] = i < nz ? __ldg(xv + s_col[x0 + i - col_base]) : (X)0;
+            }
+            Acc acc;
+            acc.zero();
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                const int i = lane + 32 * j;
+                if (i < nz) acc.add(to_p(s_val[x0 + i - val_base]) * (P)xg[j]);
+            }
+            double v = acc.value();
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            Y* __restrict__ y = static_cast<Y*>(a.y);
+            resolve_swap(pa, y, a.alpha, a.beta);
+            resolve_swap(pb, y, a.alpha, a.beta);
+            if (lane == 31) {
+                publish_carry(a.slots, a.nslots, epoch, u, v);
+                // the row may have begun in this tile and end in the next
+                const int rs1 = s_rp[rpo0];
+                if (y1 < a.nrow && u + 1 < a.num_tiles && rs1 >= x0 && rs1 < x1) {
+                    pa.got = swap_boundary(a.xch, a.nslots, epoch, u + 1, v);
+                    pa.mine = v;
+                    pa.row = y1;
+                    pa.carry = 1;
+                }
+            }
+            return;
+        }
 
         // ---- products, in place of the staged values (or of col when the
         // product is wider than a value)
