@@ -133,6 +133,25 @@ int merbit_plan_config_usable(merbit_plan plan, int32_t idx, int32_t* usable, vo
 int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
                 void* stream);
 
+/* ---------------- adjoint (differentiation) ---------------- */
+
+/* Builds the plan of A^T (ncol x nrow) from a plan of A: a stable sort of
+ * the column indices (so every A^T row keeps A's row order and dX sums are
+ * taken in a fixed order), the transposed structure and a gathered copy of
+ * the values, all owned by the new plan.  dX = A^T G is then
+ * merbit_spmm(tplan, ...).  The source plan must outlive nothing here: the
+ * transpose owns its arrays.  Synchronizes. */
+int merbit_plan_transpose(merbit_plan plan, merbit_plan* tplan, void* stream);
+/* Re-gathers the transpose's values after A's values changed (same
+ * structure): d_src_vals is A's value array. */
+int merbit_plan_transpose_refresh(merbit_plan tplan, const void* d_src_vals, void* stream);
+/* Gradient of the values: dval[e] = sum_{j<k} G[row_e, j] * X[col_e, j]
+ * (row-major G [nrow x ldg], X [ncol x ldx]; dval in the x/y type: f64 for
+ * f64 plans, f32 otherwise).  Each sum in a fixed order, no atomics.  The
+ * first call builds the plan's nonzero-to-row map (allocates). */
+int merbit_dval(merbit_plan plan, int32_t k, const void* d_g, int64_t ldg, const void* d_x,
+                int64_t ldx, void* d_dval, void* stream);
+
 /* ---------------- k right-hand sides and batches ---------------- */
 
 /* Y[nrow x k] = alpha*A*X[ncol x k] + beta*Y, row-major with leading

@@ -76,6 +76,9 @@ SIGNATURES = {
     "merbit_plan_set_config": (C.c_int, [_P, C.c_int32, _P]),
     "merbit_plan_config_usable": (C.c_int, [_P, C.c_int32, _P, _P]),
     "merbit_plan_check": (C.c_int, [_P, _P]),
+    "merbit_plan_transpose": (C.c_int, [_P, _P, _P]),
+    "merbit_plan_transpose_refresh": (C.c_int, [_P, _P, _P]),
+    "merbit_dval": (C.c_int, [_P, C.c_int32, _P, C.c_int64, _P, C.c_int64, _P, _P]),
     "merbit_spmm": (C.c_int, [_P, C.c_int32, C.c_double, _P, C.c_int64, C.c_double, _P,
                               C.c_int64, _P]),
     "merbit_batch_create": (C.c_int, [_P, C.c_int32, _P, C.c_int32, _P, _P, _P, _P, _P]),

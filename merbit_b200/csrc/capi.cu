@@ -250,6 +250,8 @@ int merbit_plan_destroy(merbit_plan plan) {
     }
     cudaFree(plan->carry);
     cudaFree(plan->state);
+    cudaFree(plan->row_of);
+    for (void* q : plan->owned) cudaFree(q);
     delete plan;
     return MERBIT_OK;
 }

@@ -423,6 +423,12 @@ struct merbit_plan_s {
     merbit::LaunchState* state = nullptr;
     // SpMM carry slots, keyed by (k << 20 | tile items)
     std::map<long long, merbit::SpmmSlots> spmm_slots;
+    // adjoint support: row index of every nonzero (built on first use), and
+    // for a transpose plan the permutation into the source's nonzeros plus
+    // the device buffers the plan owns (col_ptr, row_idx, perm, values)
+    int* row_of = nullptr;
+    int* perm = nullptr;
+    std::vector<void*> owned;
 };
 
 namespace merbit {

@@ -284,6 +284,33 @@ int orc_spmv_omp_f64(int64_t nrow, const int32_t* row_ptr, const int32_t* col,
     return nthreads;
 }
 
+/* Row-parallel OpenMP CSR SpMM in float (values f32, X/Y f32 row-major,
+ * k columns, double accumulation per output): the CPU baseline of the
+ * batched form.  Returns the number of threads used. */
+int orc_spmm_omp_f32(int64_t nrow, const int32_t* row_ptr, const int32_t* col,
+                     const float* vals, const float* x, int64_t k, float* y, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads)
+    for (int64_t i = 0; i < nrow; ++i) {
+        double acc[64];
+        for (int64_t j0 = 0; j0 < k; j0 += 64) {
+            const int64_t kk = k - j0 < 64 ? k - j0 : 64;
+            for (int64_t j = 0; j < kk; ++j) acc[j] = 0.0;
+            for (int64_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e) {
+                const double a = vals[e];
+                const float* xr = x + (int64_t)col[e] * k + j0;
+                for (int64_t j = 0; j < kk; ++j) acc[j] += a * xr[j];
+            }
+            for (int64_t j = 0; j < kk; ++j) y[i * k + j0 + j] = (float)acc[j];
+        }
+    }
+    return nthreads;
+}
+
 int orc_max_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

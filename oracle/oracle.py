@@ -56,6 +56,8 @@ def lib():
         L.orc_spmv_omp_f64.argtypes = [_i64, _p, _p, _p, _p, _p, C.c_int]
         L.orc_spmv_omp_f64.restype = C.c_int
         L.orc_max_threads.restype = C.c_int
+        L.orc_spmm_omp_f32.argtypes = [_i64, _p, _p, _p, _p, _i64, _p, C.c_int]
+        L.orc_spmm_omp_f32.restype = C.c_int
         _lib = L
     return _lib
 
@@ -188,6 +190,16 @@ def spmv_omp_f64(row_ptr, col, vals, x, y=None, nthreads: int = 0):
         y = np.empty(nrow, np.float64)
     n = lib().orc_spmv_omp_f64(nrow, _ptr(row_ptr), _ptr(col), _ptr(vals), _ptr(x), _ptr(y),
                                nthreads)
+    return y, n
+
+
+def spmm_omp_f32(row_ptr, col, vals32, x32, k: int, y=None, nthreads: int = 0):
+    """Row-parallel OpenMP float SpMM (batched-form CPU baseline)."""
+    nrow = len(row_ptr) - 1
+    if y is None:
+        y = np.empty((nrow, k), np.float32)
+    n = lib().orc_spmm_omp_f32(nrow, _ptr(row_ptr), _ptr(col), _ptr(vals32), _ptr(x32), k,
+                               _ptr(y), nthreads)
     return y, n
 
 
