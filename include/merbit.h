@@ -133,6 +133,23 @@ int merbit_plan_config_usable(merbit_plan plan, int32_t idx, int32_t* usable, vo
 int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
                 void* stream);
 
+/* ---------------- harness front end ---------------- */
+
+/* Sorts COO triplets in place by (major, minor) -- GRAPH::sort
+ * (src/class.cu:143-177): sort(false) orders by (col, row), i.e. major =
+ * col_ind.  Stable and deterministic.  d_vals may be NULL.  Synchronizes. */
+int merbit_coo_sort(int32_t nnz, int32_t* d_major, int32_t* d_minor, void* d_vals,
+                    merbit_dtype dtype, void* stream);
+/* row_ptr[nrow+1] of sorted row indices -- cusparseXcoo2csr as used in
+ * include/tile.cuh:574 (zero-based). */
+int merbit_coo_to_csr(int32_t nnz, const int32_t* d_sorted_rows, int32_t nrow, int32_t* d_row_ptr,
+                      void* stream);
+/* values[e] = 1 / #{e' : row_ind[e'] == row_ind[e]} -- the PageRank weights
+ * the reference loader writes over a Matrix Market file's values
+ * (Fun_Values, src/class.cu:2-34).  Synchronizes. */
+int merbit_outdegree_values(int32_t nnz, int32_t nrow, const int32_t* d_row_ind, void* d_vals,
+                            merbit_dtype dtype, void* stream);
+
 /* ---------------- adjoint (differentiation) ---------------- */
 
 /* Builds the plan of A^T (ncol x nrow) from a plan of A: a stable sort of

@@ -76,6 +76,9 @@ SIGNATURES = {
     "merbit_plan_set_config": (C.c_int, [_P, C.c_int32, _P]),
     "merbit_plan_config_usable": (C.c_int, [_P, C.c_int32, _P, _P]),
     "merbit_plan_check": (C.c_int, [_P, _P]),
+    "merbit_coo_sort": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int, _P]),
+    "merbit_coo_to_csr": (C.c_int, [C.c_int32, _P, C.c_int32, _P, _P]),
+    "merbit_outdegree_values": (C.c_int, [C.c_int32, C.c_int32, _P, _P, C.c_int, _P]),
     "merbit_plan_transpose": (C.c_int, [_P, _P, _P]),
     "merbit_plan_transpose_refresh": (C.c_int, [_P, _P, _P]),
     "merbit_dval": (C.c_int, [_P, C.c_int32, _P, C.c_int64, _P, C.c_int64, _P, _P]),
@@ -169,6 +172,49 @@ def tile_build(row_ptr: torch.Tensor, nnz: int, sigma: int = 14, stream=None):
     _check(lib().merbit_tile_build(_dptr(row_ptr), nrow, nnz, sigma, _dptr(tx), _dptr(ty),
                                    _dptr(desc), _stream_ptr(stream)))
     return tx, ty, desc[:Ln]
+
+
+_DT = {torch.float64: 0, torch.float32: 1, torch.bfloat16: 2}
+
+
+def coo_sort(major: torch.Tensor, minor: torch.Tensor, vals: torch.Tensor | None = None,
+             stream=None) -> None:
+    """Sorts COO triplets in place by (major, minor), stably -- GRAPH::sort
+    (src/class.cu:143-177) with major = col_ind for sort(false)."""
+    _need_cuda(major, "major", torch.int32)
+    _need_cuda(minor, "minor", torch.int32)
+    n = major.numel()
+    if minor.numel() != n or (vals is not None and vals.numel() != n):
+        raise ValueError("major, minor and vals must have the same length")
+    if vals is not None:
+        _need_cuda(vals, "vals")
+        if vals.dtype not in _DT:
+            raise TypeError(f"unsupported value dtype {vals.dtype}")
+    _check(lib().merbit_coo_sort(n, _dptr(major), _dptr(minor), _dptr(vals),
+                                 _DT[vals.dtype] if vals is not None else 0, _stream_ptr(stream)))
+
+
+def coo_to_csr(sorted_rows: torch.Tensor, nrow: int, stream=None) -> torch.Tensor:
+    """row_ptr[nrow+1] of a sorted row-index array (cusparseXcoo2csr as
+    include/tile.cuh:574 calls it, zero-based)."""
+    _need_cuda(sorted_rows, "sorted_rows", torch.int32)
+    rp = torch.empty(nrow + 1, dtype=torch.int32, device=sorted_rows.device)
+    _check(lib().merbit_coo_to_csr(sorted_rows.numel(), _dptr(sorted_rows), nrow, _dptr(rp),
+                                   _stream_ptr(stream)))
+    return rp
+
+
+def outdegree_values(row_ind: torch.Tensor, nrow: int, dtype=torch.float64,
+                     stream=None) -> torch.Tensor:
+    """values[e] = 1 / (entries sharing row_ind[e]) -- the loader's PageRank
+    weights (Fun_Values, src/class.cu:2-34)."""
+    _need_cuda(row_ind, "row_ind", torch.int32)
+    if dtype not in _DT:
+        raise TypeError(f"unsupported value dtype {dtype}")
+    out = torch.empty(row_ind.numel(), dtype=dtype, device=row_ind.device)
+    _check(lib().merbit_outdegree_values(row_ind.numel(), nrow, _dptr(row_ind), _dptr(out),
+                                         _DT[dtype], _stream_ptr(stream)))
+    return out
 
 
 @dataclass

@@ -25,6 +25,9 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libmerbit_b200.so")
 SYNTH = os.path.join(PKG, "libmerbit_synth.so")
+EXAMPLE_SRC = os.path.join(PKG, "compat", "merbit_main.cpp")
+EXAMPLE = os.path.join(PKG, "compat", "merbit_main")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -83,10 +86,24 @@ def build(force: bool = False, verbose: bool = False) -> None:
                 fut.result()
     if force or jobs or _stale(LIB, objs):
         _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs)
+    build_example(force)
     synth_src = os.path.join(CSRC, "synth.cpp")
     if force or _stale(SYNTH, [synth_src, os.path.join(ROOT, "include", "merbit_synth.h")]):
         _run([_hostcxx(), "-O3", "-fopenmp", "-fPIC", "-shared", "-std=c++17", "-o", SYNTH,
               synth_src])
+
+
+def build_example(force: bool = False) -> None:
+    """The C++ harness (merbit_b200/compat/merbit_main.cpp) against
+    include/merbit_compat.hpp, libmerbit_b200.so and the CUDA runtime."""
+    deps = [EXAMPLE_SRC, LIB, os.path.join(ROOT, "include", "merbit_compat.hpp"),
+            os.path.join(ROOT, "include", "merbit.h")]
+    if not (force or _stale(EXAMPLE, deps)):
+        return
+    _run([_hostcxx(), "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+          "-I", os.path.join(CUDA_HOME, "include"), EXAMPLE_SRC, "-o", EXAMPLE,
+          "-L", PKG, "-lmerbit_b200", "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart",
+          "-Wl,-rpath,$ORIGIN/..", "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64")])
 
 
 if __name__ == "__main__":
