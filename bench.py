@@ -149,21 +149,31 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(mhz)}
 
 
-def dist_setup(args):
+def dist_env():
+    """(world_size, rank, local_rank) from the torchrun environment."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def dist_setup(args, backend: str | None = None, timeout_s: float = 120.0):
+    """One process per GPU: the process group (NCCL on GPUs, gloo otherwise)
+    with a short timeout, and this rank's device."""
     import torch
 
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ws, rank, local = dist_env()
+    cuda = torch.cuda.is_available()
     if ws > 1:
         import datetime
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
+        backend = backend or ("nccl" if cuda else "gloo")
+        kw = {}
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            kw["device_id"] = torch.device("cuda", local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+    elif cuda:
         torch.cuda.set_device(0)
     return ws, rank, local
 
@@ -176,14 +186,22 @@ def barrier(ws):
 
 
 def allreduce_max(ws, v: float) -> float:
+    """The maximum of v over ranks (every rank gets it)."""
     if ws == 1:
         return v
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def weak_value(ws: int, units_per_rank: float, ms_max: float) -> float:
+    """Whole-job throughput of a weak-scaling run: every rank processed
+    units_per_rank; the job took as long as its slowest rank."""
+    return ws * units_per_rank / (ms_max * 1e-3)
 
 
 def load(args):
@@ -279,7 +297,7 @@ def run_ours(args):
         plan.spmv(xd, yd)
         b.record(stream)
     torch.cuda.synchronize(dev)
-    ms_cold = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    ms_cold = allreduce_max(ws, statistics.mean(a.elapsed_time(b) for a, b in evs))
     del flush
 
     # ---- e2e through the public API with host buffers
@@ -311,7 +329,7 @@ def run_ours(args):
         return
 
     peak, peak_src = peaks()
-    value = ws * B / (ms * 1e-3) / 1e9
+    value = weak_value(ws, B, ms) / 1e9
     achieved = B / (ms * 1e-3) / 1e9
     traffic = traffic_from_profile(args.workload, args.dtype)
     out = {
@@ -619,16 +637,15 @@ def run_diff(args):
 
 
 def run_reference(args):
+    """The reference arm: rank 0 alone times the CPU implementation; other
+    ranks exit at once (no process group, nothing to wait for)."""
     import torch
 
-    ws, rank, local = dist_setup(args)
+    ws, rank, local = dist_env()
     if rank != 0:
-        barrier(ws)
-        if ws > 1:
-            import torch.distributed as dist
-
-            dist.destroy_process_group()
         return
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
     from oracle import oracle as O
 
     A, x = load(args)
@@ -711,11 +728,6 @@ def run_reference(args):
                 "plan_build_s_host_wall": round(t_plan, 4),
             }
     print(json.dumps(out), flush=True)
-    if ws > 1:
-        barrier(ws)
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
 
 
 def main():

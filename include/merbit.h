@@ -133,6 +133,20 @@ int merbit_plan_config_usable(merbit_plan plan, int32_t idx, int32_t* usable, vo
 int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, void* d_y,
                 void* stream);
 
+/* One PageRank power step in a single launch (the iteration PARAMETER's
+ * damp / perrnd / maxiter scaffold, include/class.cuh:119-146; the residual
+ * is RESULT::norm, include/class.cuh:157):
+ *     y = damp * A x + (1 - damp) * teleport
+ *     *d_residual = sum_i |y_i - x_i|   (L1, of y as stored; skipped if NULL)
+ * The residual is reduced inside the SpMV launch -- per-CTA partials summed in
+ * a fixed order by the launch's last CTA -- so it is deterministic and costs
+ * no extra pass over y.  The plan must be square; x, teleport and y are
+ * vectors of the plan's x/y type; y must not alias x (teleport may alias y).
+ * A row without nonzeros gets only the teleport term; the rank of a node
+ * without out-links is not redistributed (plain power step). */
+int merbit_pagerank_step(merbit_plan plan, double damp, const void* d_x, const void* d_teleport,
+                         void* d_y, double* d_residual, void* stream);
+
 /* ---------------- harness front end ---------------- */
 
 /* Sorts COO triplets in place by (major, minor) -- GRAPH::sort
@@ -231,6 +245,14 @@ int merbit_spmv_noalloc(int32_t nrow, int32_t ncol, int32_t nnz, const int32_t* 
 /* Reads and clears the plan's device-side status (MERBIT_ERR_TIMEOUT if a
  * carry wait ran out in any launch since the last check).  Synchronizes. */
 int merbit_plan_check(merbit_plan plan, void* stream);
+
+/* Failure-detection self-test (no reference counterpart): runs one bounded
+ * device wait of the kind the kernels use -- which = 0 the cross-CTA carry
+ * wait, 1 the shared-memory mbarrier wait of the staged copies -- on a flag
+ * that nothing sets, with a limit of wait_us microseconds (1 .. 1e6).  The
+ * wait runs out, records MERBIT_ERR_TIMEOUT in the plan's device status and
+ * returns; merbit_plan_check then reports it.  No fault, trap or hang. */
+int merbit_plan_selftest_wait(merbit_plan plan, int32_t which, int32_t wait_us, void* stream);
 
 /* ---------------- errors ---------------- */
 

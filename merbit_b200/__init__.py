@@ -76,6 +76,8 @@ SIGNATURES = {
     "merbit_plan_set_config": (C.c_int, [_P, C.c_int32, _P]),
     "merbit_plan_config_usable": (C.c_int, [_P, C.c_int32, _P, _P]),
     "merbit_plan_check": (C.c_int, [_P, _P]),
+    "merbit_pagerank_step": (C.c_int, [_P, C.c_double, _P, _P, _P, _P, _P]),
+    "merbit_plan_selftest_wait": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
     "merbit_coo_sort": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int, _P]),
     "merbit_coo_to_csr": (C.c_int, [C.c_int32, _P, C.c_int32, _P, _P]),
     "merbit_outdegree_values": (C.c_int, [C.c_int32, C.c_int32, _P, _P, C.c_int, _P]),
@@ -174,9 +176,6 @@ def tile_build(row_ptr: torch.Tensor, nnz: int, sigma: int = 14, stream=None):
     return tx, ty, desc[:Ln]
 
 
-_DT = {torch.float64: 0, torch.float32: 1, torch.bfloat16: 2}
-
-
 def coo_sort(major: torch.Tensor, minor: torch.Tensor, vals: torch.Tensor | None = None,
              stream=None) -> None:
     """Sorts COO triplets in place by (major, minor), stably -- GRAPH::sort
@@ -188,10 +187,10 @@ def coo_sort(major: torch.Tensor, minor: torch.Tensor, vals: torch.Tensor | None
         raise ValueError("major, minor and vals must have the same length")
     if vals is not None:
         _need_cuda(vals, "vals")
-        if vals.dtype not in _DT:
+        if vals.dtype not in _DT_OF:
             raise TypeError(f"unsupported value dtype {vals.dtype}")
     _check(lib().merbit_coo_sort(n, _dptr(major), _dptr(minor), _dptr(vals),
-                                 _DT[vals.dtype] if vals is not None else 0, _stream_ptr(stream)))
+                                 _DT_OF[vals.dtype] if vals is not None else 0, _stream_ptr(stream)))
 
 
 def coo_to_csr(sorted_rows: torch.Tensor, nrow: int, stream=None) -> torch.Tensor:
@@ -209,11 +208,11 @@ def outdegree_values(row_ind: torch.Tensor, nrow: int, dtype=torch.float64,
     """values[e] = 1 / (entries sharing row_ind[e]) -- the loader's PageRank
     weights (Fun_Values, src/class.cu:2-34)."""
     _need_cuda(row_ind, "row_ind", torch.int32)
-    if dtype not in _DT:
+    if dtype not in _DT_OF:
         raise TypeError(f"unsupported value dtype {dtype}")
     out = torch.empty(row_ind.numel(), dtype=dtype, device=row_ind.device)
     _check(lib().merbit_outdegree_values(row_ind.numel(), nrow, _dptr(row_ind), _dptr(out),
-                                         _DT[dtype], _stream_ptr(stream)))
+                                         _DT_OF[dtype], _stream_ptr(stream)))
     return out
 
 
@@ -306,6 +305,25 @@ class Plan:
                                  _stream_ptr(stream)))
         return y
 
+    def pagerank_step(self, x: torch.Tensor, teleport: torch.Tensor, damp: float = 0.85,
+                      y: torch.Tensor | None = None, residual: torch.Tensor | None = None,
+                      stream=None) -> torch.Tensor:
+        """y = damp*A*x + (1-damp)*teleport in one launch; when `residual` (a
+        float64 CUDA tensor of one element) is given it receives
+        sum|y - x| from the same launch."""
+        self._vec(x, self.ncol, "x")
+        self._vec(teleport, self.nrow, "teleport")
+        if y is None:
+            y = torch.empty(self.nrow, dtype=self.xy_dtype, device=self.device)
+        else:
+            self._vec(y, self.nrow, "y")
+        if residual is not None and (not residual.is_cuda or residual.dtype != torch.float64
+                                     or residual.numel() < 1):
+            raise TypeError("residual must be a float64 CUDA tensor with one element")
+        _check(lib().merbit_pagerank_step(self._h, float(damp), _dptr(x), _dptr(teleport),
+                                          _dptr(y), _dptr(residual), _stream_ptr(stream)))
+        return y
+
     def _mat(self, t: torch.Tensor, rows: int, name: str) -> int:
         if not t.is_cuda or t.dtype != self.xy_dtype:
             raise TypeError(f"{name} must be a CUDA {self.xy_dtype} tensor")
@@ -356,6 +374,11 @@ class Plan:
     def check(self, stream=None) -> None:
         """Raise MerbitError if a device-side wait of any launch ran out."""
         _check(lib().merbit_plan_check(self._h, _stream_ptr(stream)))
+
+    def selftest_wait(self, which: int = 0, wait_us: int = 2000, stream=None) -> None:
+        """Launch one bounded device wait (0: carry, 1: mbarrier) on a flag
+        nothing sets; the next check() raises MERBIT_ERR_TIMEOUT."""
+        _check(lib().merbit_plan_selftest_wait(self._h, which, wait_us, _stream_ptr(stream)))
 
 
 class _BatchInfo(C.Structure):
@@ -411,3 +434,35 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def pagerank(plan: Plan, damp: float = 0.85, tol: float = 1e-10, maxiter: int = 100,
+             perrnd: int = 1, teleport: torch.Tensor | None = None,
+             x0: torch.Tensor | None = None):
+    """Power iteration x <- damp*A*x + (1-damp)*teleport on a square plan,
+    with the PARAMETER scaffold's knobs (include/class.cuh:119-146): at most
+    `maxiter` rounds of `perrnd` fused steps each; the L1 residual of the
+    last step of a round is read on the host once per round and iteration
+    stops when it is <= tol.  teleport defaults to the uniform 1/n vector,
+    x0 to teleport.  Returns (x, steps, residual per round)."""
+    n = plan.nrow
+    if plan.ncol != n:
+        raise ValueError("pagerank needs a square plan")
+    dt = plan.xy_dtype
+    if teleport is None:
+        teleport = torch.full((n,), 1.0 / max(n, 1), dtype=dt, device=plan.device)
+    x = (teleport if x0 is None else x0).clone()
+    y = torch.empty_like(x)
+    res = torch.zeros(1, dtype=torch.float64, device=plan.device)
+    history = []
+    steps = 0
+    for _ in range(maxiter):
+        for _ in range(perrnd):
+            plan.pagerank_step(x, teleport, damp, y=y, residual=res)
+            x, y = y, x
+            steps += 1
+        r = float(res.item())
+        history.append(r)
+        if r <= tol:
+            break
+    return x, steps, history

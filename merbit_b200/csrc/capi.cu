@@ -4,6 +4,7 @@
 // (include/tile.cuh:563-615: offset build, TILE construction, y/z buffers),
 // done once and reused: the partition for the chosen tile size and the
 // carry slots stay resident in HBM across launches.
+#include <algorithm>
 #include <chrono>
 #include <map>
 #include <mutex>
@@ -94,12 +95,34 @@ int plan_pick_default(merbit_plan_s* p, cudaStream_t s) {
     return fail(MERBIT_ERR_UNSUPPORTED, "no SpMV configuration fits this matrix");
 }
 
+// Grows the plan's residual partials to hold one word per CTA of any launch
+// over `num_tiles` tiles (warp-tile kernel: at most 32 resident CTAs per SM;
+// CTA-tile kernel: one CTA per tile).
+int plan_partials(merbit_plan_s* p, int num_tiles) {
+    int sms = 0;
+    MERBIT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
+    const long long need = std::max<long long>(num_tiles, 32LL * std::max(sms, 1));
+    if (need <= p->npartials) return MERBIT_OK;
+    cudaFree(p->partials);
+    p->partials = nullptr;
+    p->npartials = 0;
+    MERBIT_CUDA(cudaMalloc(&p->partials, sizeof(double) * (size_t)need));
+    p->npartials = need;
+    return MERBIT_OK;
+}
+
+// y = alpha A x + beta z (z NULL: y); residual != NULL also writes
+// *residual = sum_r |y[r] - x[r]| from the same launch.
 int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta, void* y,
-             cudaStream_t s) {
+             cudaStream_t s, const void* z = nullptr, double* residual = nullptr) {
     const SpmvConfig c = spmv_config(p->dtype, cfg);
     const Partition* part = nullptr;
     int st = plan_partition(p, spmv_tile_items(c), &part, s);
     if (st != MERBIT_OK) return st;
+    if (residual) {
+        st = plan_partials(p, part->num_tiles);
+        if (st != MERBIT_OK) return st;
+    }
     SpmvLaunch a;
     a.row_ptr = p->row_ptr;
     a.col = p->col;
@@ -116,6 +139,12 @@ int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta
     a.num_tiles = part->num_tiles;
     a.alpha = alpha;
     a.beta = beta;
+    a.z = z;
+    if (residual) {
+        a.xres = x;
+        a.partials = p->partials;
+        a.residual = residual;
+    }
     return spmv_launch(p->dtype, cfg, p->vec, a, s);
 }
 
@@ -251,6 +280,7 @@ int merbit_plan_destroy(merbit_plan plan) {
     cudaFree(plan->carry);
     cudaFree(plan->state);
     cudaFree(plan->row_of);
+    cudaFree(plan->partials);
     for (void* q : plan->owned) cudaFree(q);
     delete plan;
     return MERBIT_OK;
@@ -298,6 +328,22 @@ int merbit_spmv(merbit_plan plan, double alpha, const void* d_x, double beta, vo
     if (plan->nrow == 0) return MERBIT_OK;
     if (!d_y || (plan->ncol > 0 && !d_x)) return fail(MERBIT_ERR_INVALID, "spmv: x/y is null");
     return run_spmv(plan, plan->cfg, alpha, d_x, beta, d_y, (cudaStream_t)stream);
+}
+
+int merbit_pagerank_step(merbit_plan plan, double damp, const void* d_x, const void* d_teleport,
+                         void* d_y, double* d_residual, void* stream) {
+    if (!plan) return fail(MERBIT_ERR_INVALID, "pagerank_step: plan is null");
+    if (plan->nrow != plan->ncol) return fail(MERBIT_ERR_INVALID, "pagerank_step: plan is not square");
+    if (plan->nrow == 0) {
+        if (d_residual) MERBIT_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(double), (cudaStream_t)stream));
+        return MERBIT_OK;
+    }
+    if (!d_x || !d_y || !d_teleport) return fail(MERBIT_ERR_INVALID, "pagerank_step: null vector");
+    if (d_x == d_y) return fail(MERBIT_ERR_INVALID, "pagerank_step: x and y must differ");
+    if (!(damp >= 0.0 && damp <= 1.0)) return fail(MERBIT_ERR_INVALID, "pagerank_step: damp outside [0, 1]");
+    MERBIT_CUDA(cudaSetDevice(plan->device));
+    return run_spmv(plan, plan->cfg, damp, d_x, 1.0 - damp, d_y, (cudaStream_t)stream, d_teleport,
+                    d_residual);
 }
 
 int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream) {

@@ -92,16 +92,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 // raises MERBIT_ERR_TIMEOUT, waits once more (bounded) for the copies still
 // in flight, and returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase,
-                                                  LaunchState* st) {
+                                                  LaunchState* st,
+                                                  unsigned long long wait_ns = kCarryWaitNs) {
     if (mbar_try_wait(bar, phase)) return true;
     unsigned long long t0 = global_timer_ns();
     for (;;) {
         if (mbar_try_wait(bar, phase)) return true;
-        if (global_timer_ns() - t0 > kCarryWaitNs) break;
+        if (global_timer_ns() - t0 > wait_ns) break;
     }
     atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
     t0 = global_timer_ns();
-    while (!mbar_try_wait(bar, phase) && global_timer_ns() - t0 < kCarryWaitNs) {
+    while (!mbar_try_wait(bar, phase) && global_timer_ns() - t0 < wait_ns) {
     }
     return false;
 }
@@ -153,7 +154,8 @@ __device__ __forceinline__ void publish_carry(unsigned long long* slots, int nsl
 
 // Reads tile t's carry, waiting (bounded) until it is published.
 __device__ __forceinline__ double read_carry(const unsigned long long* slots, int nslots,
-                                             unsigned epoch, int t, LaunchState* st) {
+                                             unsigned epoch, int t, LaunchState* st,
+                                             unsigned long long wait_ns = kCarryWaitNs) {
     const unsigned long long* p = slots + (size_t)(epoch & 1u) * nslots + t;
     unsigned long long b = ld_relaxed_u64(p);
     if (b != kEmpty) return __longlong_as_double((long long)b);
@@ -163,7 +165,7 @@ __device__ __forceinline__ double read_carry(const unsigned long long* slots, in
         b = ld_relaxed_u64(p);
         if (b != kEmpty) return __longlong_as_double((long long)b);
         if (*(volatile int*)&st->error != 0) return 0.0;
-        if (global_timer_ns() - t0 > kCarryWaitNs) {
+        if (global_timer_ns() - t0 > wait_ns) {
             atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
             return 0.0;
         }
@@ -370,8 +372,92 @@ struct SpmvLaunch {
     int num_tiles;
     int nslots;
     double alpha, beta;
+    // Fused epilogue (PageRank step).  z: the vector beta multiplies (NULL:
+    // y itself).  residual != NULL: the launch also writes
+    // *residual = sum_r |y[r] - xres[r]|, reduced through partials[] (one
+    // word per CTA of the warp-tile kernel, per tile of the CTA-tile kernel)
+    // in a fixed order by the launch's last CTA.
+    const void* z = nullptr;
+    const void* xres = nullptr;
+    double* partials = nullptr;
+    double* residual = nullptr;
 };
 int spmv_launch(int dtype, int cfg, bool vec, const SpmvLaunch& a, cudaStream_t s);
+
+// Final store of one row: y[r] = fma(beta, z[r], alpha * v) (z is y for a plain
+// product; beta == 0 reads nothing).  RES adds |y[r] - xres[r]| of the value
+// as stored to the thread's running residual.
+template <typename Y, bool RES>
+struct RowStore {
+    Y* y;
+    const Y* z;
+    const Y* xres;
+    double alpha, beta;
+    double res;
+    __device__ __forceinline__ explicit RowStore(const SpmvLaunch& a)
+        : y(static_cast<Y*>(a.y)),
+          z(static_cast<const Y*>(a.z ? a.z : a.y)),
+          xres(static_cast<const Y*>(a.xres)),
+          alpha(a.alpha),
+          beta(a.beta),
+          res(0.0) {}
+    // explicit roundings: every kernel instantiation stores the same bits
+    __device__ __forceinline__ void operator()(int r, double v) {
+        double o = __dmul_rn(alpha, v);
+        if (beta != 0.0) o = __fma_rn(beta, (double)z[r], o);
+        const Y yo = (Y)o;
+        y[r] = yo;
+        if (RES) res += fabs((double)yo - (double)xres[r]);
+    }
+};
+
+// finish_launch for a launch that reduces a residual: called by every thread
+// of the CTA with its running residual `v`.  The CTA's sum (butterfly, then
+// warps in order) goes to partials[idx]; the launch's last CTA sums
+// partials[0, nparts) in a fixed order into *out, then resets the launch
+// state as finish_launch does.  The result does not depend on timing.
+template <int NW>
+__device__ __forceinline__ void finish_launch_residual(LaunchState* st, unsigned epoch, double v,
+                                                       double* partials, int idx, int nparts,
+                                                       double* out) {
+    __shared__ double s_red[NW];
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if (lane == 0) s_red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) t += s_red[w];
+        partials[idx] = t;
+        __threadfence();
+        const unsigned prev = atomicAdd(&st->done, 1u);
+        s_last = prev == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double t = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += NW * 32)
+        t += __longlong_as_double((long long)ld_relaxed_u64(
+            reinterpret_cast<const unsigned long long*>(partials + i)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
+    if (lane == 0) s_red[warp] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) tot += s_red[w];
+        *out = tot;
+        st->ticket = 0ull;
+        st->done = 0u;
+        __threadfence();
+        *(volatile unsigned*)&st->epoch = epoch + 1u;
+    }
+}
 
 // One matrix of an SpMM launch (spmm.cu).  Tiles of ITEMS merge items;
 // coords are the matrix's own partition (local tile indices), tile_begin
@@ -429,6 +515,9 @@ struct merbit_plan_s {
     int* row_of = nullptr;
     int* perm = nullptr;
     std::vector<void*> owned;
+    // per-CTA residual partials of the fused PageRank step (grown on use)
+    double* partials = nullptr;
+    long long npartials = 0;
 };
 
 namespace merbit {

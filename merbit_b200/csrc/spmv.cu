@@ -34,7 +34,7 @@ struct SpmvSmem {
     static constexpr size_t bytes = prod_bytes + rows_bytes + rp_bytes;
 };
 
-template <int DT, int BLOCK, int IPT, bool VEC>
+template <int DT, int BLOCK, int IPT, bool VEC, bool RES>
 __global__ void __launch_bounds__(BLOCK) spmv_tile_kernel(const SpmvLaunch a) {
     using Pr = Prec<DT>;
     using V = typename Pr::V;
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(BLOCK) spmv_tile_kernel(const SpmvLaunch a) {
     if (t >= a.num_tiles) {  // launch bookkeeping out of step: report, touch nothing
         if (tid == 0) {
             atomicExch(&a.state->error, (int)MERBIT_ERR_TIMEOUT);
-            finish_launch(a.state, epoch);
+            finish_launch(a.state, epoch);  // the residual, if any, is not written
         }
         return;
     }
@@ -234,16 +234,18 @@ __global__ void __launch_bounds__(BLOCK) spmv_tile_kernel(const SpmvLaunch a) {
     __syncthreads();
 
     // ---- write the rows that end in this tile, coalesced
-    Y* __restrict__ y = static_cast<Y*>(a.y);
+    RowStore<Y, RES> out(a);
     for (int i = tid; i < nr; i += BLOCK) {
         double r = s_rows[i];
         if (i == 0 && need_lb) r = s_carry + r;
-        r *= a.alpha;
-        if (a.beta != 0.0) r += a.beta * (double)y[y0 + i];
-        y[y0 + i] = (Y)r;
+        out(y0 + i, r);
     }
 
-    if (tid == 0) finish_launch(a.state, epoch);
+    if (RES)
+        finish_launch_residual<NW>(a.state, epoch, out.res, a.partials, t, a.num_tiles,
+                                   a.residual);
+    else if (tid == 0)
+        finish_launch(a.state, epoch);
 }
 
 // ---------------------------------------------------------------------------
@@ -263,23 +265,30 @@ constexpr SpmvConfig kCfgF32[] = {
     {1, 256, 15, 1}, {1, 128, 15, 1}, {1, 256, 11, 1}, {1, 256, 7, 1}, {1, 128, 23, 1},
     {1, 128, 15, 2}, {1, 128, 7, 2},  {0, 256, 11, 1}, {0, 256, 7, 1},  {0, 256, 15, 1}};
 
-template <int DT, int BLOCK, int IPT, bool VEC>
-int launch_one(const SpmvLaunch& a, cudaStream_t s) {
+template <int DT, int BLOCK, int IPT, bool VEC, bool RES>
+int launch_one_k(const SpmvLaunch& a, cudaStream_t s) {
     using P = typename Prec<DT>::P;
     constexpr size_t smem = SpmvSmem<BLOCK, IPT, P>::bytes;
     static bool attr_set[64] = {};  // per device ordinal
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(spmv_tile_kernel<DT, BLOCK, IPT, VEC>,
+        cudaError_t e = cudaFuncSetAttribute(spmv_tile_kernel<DT, BLOCK, IPT, VEC, RES>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(spmv)");
         attr_set[dev] = true;
     }
-    spmv_tile_kernel<DT, BLOCK, IPT, VEC><<<a.num_tiles, BLOCK, smem, s>>>(a);
+    spmv_tile_kernel<DT, BLOCK, IPT, VEC, RES><<<a.num_tiles, BLOCK, smem, s>>>(a);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? (int)MERBIT_OK : cuda_fail(e, "spmv_tile_kernel launch");
+}
+
+template <int DT, int BLOCK, int IPT, bool VEC>
+int launch_one(const SpmvLaunch& a, cudaStream_t s) {
+    if (a.residual && !a.partials) return fail(MERBIT_ERR_INVALID, "spmv: residual without partials");
+    return a.residual ? launch_one_k<DT, BLOCK, IPT, VEC, true>(a, s)
+                      : launch_one_k<DT, BLOCK, IPT, VEC, false>(a, s);
 }
 
 template <int DT, int BLOCK, int IPT>

@@ -66,14 +66,6 @@ struct WarpSmem {
     static constexpr size_t bytes = bar_offset + 16;
 };
 
-template <typename Y>
-__device__ __forceinline__ void store_row(Y* __restrict__ y, int r, double v, double alpha,
-                                          double beta) {
-    double o = alpha * v;
-    if (beta != 0.0) o += beta * (double)y[r];
-    y[r] = (Y)o;
-}
-
 // Bytes the bulk part of stage_range moves for [s, e) of an n-element array
 // with G elements per 16 bytes.
 __device__ __forceinline__ unsigned bulk_bytes(int s, int e, int n, int G, int esz) {
@@ -119,13 +111,12 @@ struct PendingSwap {
     int carry;    // 1: `mine` is the carry (earlier tile), 0: the head (later tile)
 };
 
-template <typename Y>
-__device__ __forceinline__ void resolve_swap(PendingSwap& p, Y* __restrict__ y, double alpha,
-                                             double beta) {
+template <class RS>
+__device__ __forceinline__ void resolve_swap(PendingSwap& p, RS& out) {
     if (p.row >= 0 && p.got != kEmpty) {
         const double other = __longlong_as_double((long long)p.got);
         // always carry + head, whichever side finishes the row
-        store_row(y, p.row, p.carry ? p.mine + other : other + p.mine, alpha, beta);
+        out(p.row, p.carry ? p.mine + other : other + p.mine);
     }
     p.row = -1;
 }
@@ -170,9 +161,10 @@ struct WarpTile {
     }
 
     // Processes tile u from stage `ws` (its copies complete).
+    template <class RS>
     static __device__ __forceinline__ void process(const SpmvLaunch& a, int u, unsigned epoch,
                                                    unsigned char* ws, int lane,
-                                                   PendingSwap& pa, PendingSwap& pb) {
+                                                   PendingSwap& pa, PendingSwap& pb, RS& out) {
         const int* s_rp = reinterpret_cast<const int*>(ws);
         const int* s_col = reinterpret_cast<const int*>(ws + S::rp_bytes);
         const V* s_val = reinterpret_cast<const V*>(ws + S::rp_bytes + S::col_bytes);
@@ -208,9 +200,8 @@ struct WarpTile {
             double v = acc.value();
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-            Y* __restrict__ y = static_cast<Y*>(a.y);
-            resolve_swap(pa, y, a.alpha, a.beta);
-            resolve_swap(pb, y, a.alpha, a.beta);
+            resolve_swap(pa, out);
+            resolve_swap(pb, out);
             if (lane == 31) {
                 publish_carry(a.slots, a.nslots, epoch, u, v);
                 // the row may have begun in this tile and end in the next
@@ -276,8 +267,6 @@ struct WarpTile {
         int ly = lo, lx = dl - lo;
 
         // ---- walk IPT items: predicated steps, completed rows staged
-        Y* __restrict__ y = static_cast<Y*>(a.y);
-        const double alpha = a.alpha, beta = a.beta;
         Acc acc;
         acc.zero();
         int first_row = -1;
@@ -296,7 +285,7 @@ struct WarpTile {
                 } else if (ly < kOutCap) {
                     s_out[ly] = v;
                 } else {
-                    store_row(y, y0 + ly, v, alpha, beta);
+                    out(y0 + ly, v);
                 }
                 acc.zero();
                 ++ly;
@@ -328,13 +317,13 @@ struct WarpTile {
             if (first_row < kOutCap)
                 s_out[first_row] = rv;
             else
-                store_row(y, y0 + first_row, rv, alpha, beta);
+                out(y0 + first_row, rv);
         }
 
         // ---- trailing partial of row y1: published for long-row look-backs,
         // swapped with tile u+1 when row y1 began in this tile
-        resolve_swap(pa, y, alpha, beta);  // the previous tile's swaps
-        resolve_swap(pb, y, alpha, beta);
+        resolve_swap(pa, out);  // the previous tile's swaps
+        resolve_swap(pb, out);
         if (lane == 31) {
             publish_carry(a.slots, a.nslots, epoch, u, v);
             if (y1 < a.nrow && u + 1 < a.num_tiles) {
@@ -353,7 +342,7 @@ struct WarpTile {
         // finished below)
         const int nst = min(nr, kOutCap);
         for (int r = lane; r < nst; r += 32)
-            if (!(r == 0 && need_lb)) store_row(y, y0 + r, s_out[r], alpha, beta);
+            if (!(r == 0 && need_lb)) out(y0 + r, s_out[r]);
 
         // ---- row y0 when it began in an earlier tile
         if (need_lb) {
@@ -368,13 +357,13 @@ struct WarpTile {
             } else {
                 const double total =
                     look_back(a.coords, a.slots, a.nslots, epoch, a.state, u, rs, lane);
-                if (holds_first) store_row(y, y0, total + rv, alpha, beta);
+                if (holds_first) out(y0, total + rv);
             }
         }
     }
 };
 
-template <int DT, int WARPS, int IPT, int STAGES>
+template <int DT, int WARPS, int IPT, int STAGES, bool RES>
 __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch a) {
     using T = WarpTile<DT, IPT>;
     using S = typename T::S;
@@ -398,6 +387,7 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch 
     reset_other_parity(a.xch, a.nslots, epoch);
     const int nw = (int)gridDim.x * WARPS;
     unsigned phases = 0u;
+    RowStore<typename T::Y, RES> out(a);
     PendingSwap pa, pb;
     pa.row = pb.row = -1;
     pa.got = pb.got = kEmpty;
@@ -420,33 +410,35 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch 
             __all_sync(0xFFFFFFFFu, mbar_wait_bounded(cbar, (phases >> k) & 1u, a.state));
         phases ^= 1u << k;
         __syncwarp();
-        if (ok) T::process(a, u, epoch, cur, lane, pa, pb);
+        if (ok) T::process(a, u, epoch, cur, lane, pa, pb, out);
         if (STAGES == 1) {
             if (un < a.num_tiles) T::issue(a, un, cur, cbar, lane);
         } else {
             k ^= 1;
         }
     }
-    {
-        using Y = typename T::Y;
-        Y* y = static_cast<Y*>(a.y);
-        resolve_swap(pa, y, a.alpha, a.beta);
-        resolve_swap(pb, y, a.alpha, a.beta);
+    resolve_swap(pa, out);
+    resolve_swap(pb, out);
+    if (RES) {
+        finish_launch_residual<WARPS>(a.state, epoch, out.res, a.partials, (int)blockIdx.x,
+                                      (int)gridDim.x, a.residual);
+    } else {
+        __syncthreads();
+        if (threadIdx.x == 0) finish_launch(a.state, epoch);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) finish_launch(a.state, epoch);
 }
 
 namespace {
-template <int DT, int WARPS, int IPT, int STAGES>
-int launch_warp(const SpmvLaunch& a, cudaStream_t s) {
+template <int DT, int WARPS, int IPT, int STAGES, bool RES>
+int launch_warp_k(const SpmvLaunch& a, cudaStream_t s) {
     using S = WarpSmem<typename Prec<DT>::V, typename Prec<DT>::P, IPT>;
     constexpr size_t smem = S::bytes * WARPS * STAGES;
     static int grid_cap[64] = {};  // resident CTAs per device, from the occupancy calculator
+    if (RES && !a.partials) return fail(MERBIT_ERR_INVALID, "spmv_warp: residual without partials");
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmv_warp: device ordinal >= 64");
-    auto kern = spmv_warp_kernel<DT, WARPS, IPT, STAGES>;
+    auto kern = spmv_warp_kernel<DT, WARPS, IPT, STAGES, RES>;
     if (grid_cap[dev] == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -472,6 +464,12 @@ int launch_warp(const SpmvLaunch& a, cudaStream_t s) {
     cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
     if (e == cudaSuccess) e = cudaGetLastError();
     return e == cudaSuccess ? (int)MERBIT_OK : cuda_fail(e, "spmv_warp_kernel launch");
+}
+
+template <int DT, int WARPS, int IPT, int STAGES>
+int launch_warp(const SpmvLaunch& a, cudaStream_t s) {
+    return a.residual ? launch_warp_k<DT, WARPS, IPT, STAGES, true>(a, s)
+                      : launch_warp_k<DT, WARPS, IPT, STAGES, false>(a, s);
 }
 
 template <int DT>
