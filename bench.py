@@ -48,6 +48,7 @@ if ROOT not in sys.path:
 
 METRIC = "SpMV GB/s (% of HBM peak) & GFLOP/s; mixed/batched vs plain FP64 at 1e-6 rel"
 FALLBACK_HBM_GBS = 6650.0
+KERNEL_OF_KIND = {0: "spmv_tile_kernel", 1: "spmv_warp_kernel"}
 
 
 def parse_args():
@@ -353,10 +354,11 @@ def run_ours(args):
             "l2": "inputs larger than L2 (matrix streamed from HBM every step); "
                   "value_l2_flushed flushes L2 before every launch",
             "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-            "kernel": f"{'spmv_warp_kernel' if info.kind == 1 else 'spmv_tile_kernel'} "
+            "kernel": f"{KERNEL_OF_KIND[info.kind]} "
                       f"block={info.block} ipt={info.items_per_thread} "
                       f"tile_items={info.tile_items} tiles={info.num_tiles} "
-                      f"vectorized={int(info.vectorized)}",
+                      f"vectorized={int(info.vectorized)} l1_carveout={info.l1_carveout} "
+                      f"gather_l2_only={int(info.gather_l2_only)}",
         },
         "pct_hbm_peak": round(100.0 * achieved / peak, 2),
         "gflops": round(ws * 2.0 * A.nnz / (ms * 1e-3) / 1e9, 2),
@@ -372,7 +374,7 @@ def run_ours(args):
             "frac": round(achieved / peak, 4),
             "peak_source": f"{peak_src} hbm_gbs (copy), burst",
             "traffic": traffic,
-            "kernel": "spmv_warp_kernel" if info.kind == 1 else "spmv_tile_kernel",
+            "kernel": KERNEL_OF_KIND[info.kind],
         },
         "e2e": {
             "value": round(ws * B / (ms_e2e * 1e-3) / 1e9, 2),

@@ -54,6 +54,7 @@ class _PlanInfo(C.Structure):
         ("nrow", C.c_int32), ("ncol", C.c_int32), ("nnz", C.c_int32), ("dtype", C.c_int32),
         ("block", C.c_int32), ("items_per_thread", C.c_int32), ("tile_items", C.c_int32),
         ("num_tiles", C.c_int32), ("vectorized", C.c_int32), ("kind", C.c_int32),
+        ("l1_carveout", C.c_int32), ("gather_l2_only", C.c_int32),
         ("metadata_bytes", C.c_int64), ("algorithmic_bytes", C.c_double),
     ]
 
@@ -228,6 +229,8 @@ class PlanInfo:
     num_tiles: int
     vectorized: bool
     kind: int
+    l1_carveout: int
+    gather_l2_only: bool
     metadata_bytes: int
     algorithmic_bytes: float
 
@@ -277,8 +280,8 @@ class Plan:
         i = _PlanInfo()
         _check(lib().merbit_plan_get_info(self._h, C.byref(i)))
         return PlanInfo(i.nrow, i.ncol, i.nnz, i.dtype, i.block, i.items_per_thread,
-                        i.tile_items, i.num_tiles, bool(i.vectorized), i.kind, i.metadata_bytes,
-                        i.algorithmic_bytes)
+                        i.tile_items, i.num_tiles, bool(i.vectorized), i.kind, i.l1_carveout,
+                        bool(i.gather_l2_only), i.metadata_bytes, i.algorithmic_bytes)
 
     def set_values(self, vals: torch.Tensor) -> None:
         _need_cuda(vals, "vals", self.vals.dtype)

@@ -304,6 +304,8 @@ int merbit_plan_get_info(merbit_plan plan, merbit_plan_info* info) {
     }
     info->vectorized = plan->vec ? 1 : 0;
     info->kind = c.kind;
+    info->l1_carveout = c.carveout;
+    info->gather_l2_only = c.cg;
     info->metadata_bytes = meta;
     info->algorithmic_bytes = 4.0 * (plan->nrow + 1.0) +
                               (double)plan->nnz * (4.0 + (double)dtype_size(plan->dtype)) +

@@ -60,6 +60,21 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned by
                  "r"(bytes)
                  : "memory");
 }
+// try_wait with a suspend-time hint: a waiting warp sleeps until the phase
+// completes (or the hint runs out) instead of re-issuing the test, which
+// would keep the shared-memory instruction queue busy for the warps that have
+// work.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, unsigned phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase), "r"(100000u)
+        : "memory");
+    return ok != 0;
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
     uint32_t ok;
     asm volatile(
@@ -97,7 +112,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase,
     if (mbar_try_wait(bar, phase)) return true;
     unsigned long long t0 = global_timer_ns();
     for (;;) {
-        if (mbar_try_wait(bar, phase)) return true;
+        if (mbar_try_wait_sleep(bar, phase)) return true;
         if (global_timer_ns() - t0 > wait_ns) break;
     }
     atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
@@ -350,8 +365,17 @@ struct SpmvConfig {
     int kind;  // 0: CTA-tile kernel, 1: warp-tile kernel
     int block;
     int ipt;
-    int stages;  // warp-tile kernel: shared-memory stages per warp (1 or 2)
+    int stages;  // warp-tile kernel: shared-memory stages per warp (1)
+    // Warp-tile kernel: preferred shared-memory carveout in percent (0: the
+    // driver's choice, which for these kernels is all shared memory).  The
+    // x gathers need L1 capacity for their misses in flight; giving L1 more
+    // of the SM's 256 KB (fewer resident CTAs) pays on matrices whose
+    // gathers miss L1.
+    int carveout;
+    int cg;  // 1: x gathers cached in L2 only (ld.global.cg)
 };
+constexpr int kCarveoutL1 = 72;     // ~164 KB shared memory, the rest L1
+constexpr int kCarveoutL1Max = 58;  // ~132 KB shared memory
 int spmv_num_configs(int dtype);
 SpmvConfig spmv_config(int dtype, int idx);
 int spmv_tile_items(const SpmvConfig& c);

@@ -257,13 +257,27 @@ namespace {
 // Items per thread are odd: a lane's segment then starts an odd number of
 // elements after its neighbour's, which spreads the lanes of a warp over
 // all shared-memory banks when they walk their segments in step.
-// stages: shared-memory stages per warp of the warp-tile kernel (1 or 2).
+// stages: shared-memory stages per warp of the warp-tile kernel (the kernel
+// also runs 2, which measured slower: less occupancy and less L1).
+// Order matters only for the default pick (the first usable entry): the
+// large-L1 warp-tile entries come first because they are the better choice
+// for irregular matrices; plan_tune picks per matrix.
 constexpr SpmvConfig kCfgF64[] = {
-    {1, 256, 15, 1}, {1, 128, 15, 1}, {1, 256, 11, 1}, {1, 256, 7, 1}, {1, 128, 23, 1},
-    {1, 128, 15, 2}, {1, 128, 7, 2},  {0, 256, 7, 1},  {0, 256, 11, 1}, {0, 128, 9, 1}};
+    {1, 256, 15, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1, 1},
+    {1, 256, 11, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1Max, 1},
+    {1, 256, 15, 1, kCarveoutL1, 0}, {1, 256, 15, 1, 0, 0},
+    {1, 128, 15, 1, 0, 0},           {1, 256, 11, 1, 0, 0},
+    {1, 256, 7, 1, 0, 0},            {1, 128, 23, 1, 0, 0},
+    {0, 256, 7, 1, 0, 0},            {0, 256, 11, 1, 0, 0},
+    {0, 128, 9, 1, 0, 0}};
 constexpr SpmvConfig kCfgF32[] = {
-    {1, 256, 15, 1}, {1, 128, 15, 1}, {1, 256, 11, 1}, {1, 256, 7, 1}, {1, 128, 23, 1},
-    {1, 128, 15, 2}, {1, 128, 7, 2},  {0, 256, 11, 1}, {0, 256, 7, 1},  {0, 256, 15, 1}};
+    {1, 256, 15, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1, 1},
+    {1, 256, 11, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1Max, 1},
+    {1, 256, 15, 1, kCarveoutL1, 0}, {1, 256, 15, 1, 0, 0},
+    {1, 128, 15, 1, 0, 0},           {1, 256, 11, 1, 0, 0},
+    {1, 256, 7, 1, 0, 0},            {1, 128, 23, 1, 0, 0},
+    {0, 256, 11, 1, 0, 0},           {0, 256, 7, 1, 0, 0},
+    {0, 256, 15, 1, 0, 0}};
 
 template <int DT, int BLOCK, int IPT, bool VEC, bool RES>
 int launch_one_k(const SpmvLaunch& a, cudaStream_t s) {
@@ -317,23 +331,22 @@ SpmvConfig spmv_config(int dtype, int idx) {
     return dtype == MERBIT_F64 ? kCfgF64[idx] : kCfgF32[idx];
 }
 
-int spmv_tile_items(const SpmvConfig& c) { return c.kind == 1 ? 32 * c.ipt : c.block * c.ipt; }
+int spmv_tile_items(const SpmvConfig& c) { return c.kind != 0 ? 32 * c.ipt : c.block * c.ipt; }
 
 bool spmv_config_allowed(const SpmvConfig& c, bool vec) { return vec || c.kind == 0; }
 
 int spmv_config_row_cap(const SpmvConfig& c) {
-    return c.kind == 1 ? warp_rp_cap(c.ipt) - 8 : INT_MAX;
+    return c.kind != 0 ? warp_rp_cap(c.ipt) - 8 : INT_MAX;
 }
 
 
-int spmv_warp_launch(int dtype, int warps, int ipt, int stages, const SpmvLaunch& a,
-                     cudaStream_t s);
+int spmv_warp_launch(int dtype, const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s);
 
 int spmv_launch(int dtype, int cfg, bool vec, const SpmvLaunch& a, cudaStream_t s) {
     if (a.num_tiles <= 0) return MERBIT_OK;
     const SpmvConfig c = spmv_config(dtype, cfg);
     if (!spmv_config_allowed(c, vec)) return fail(MERBIT_ERR_INVALID, "spmv: config needs aligned arrays");
-    if (c.kind == 1) return spmv_warp_launch(dtype, c.block / 32, c.ipt, c.stages, a, s);
+    if (c.kind != 0) return spmv_warp_launch(dtype, c, a, s);
     switch (dtype) {
     case MERBIT_F64: return launch_cta<MERBIT_F64>(c.block, c.ipt, vec, a, s);
     case MERBIT_F32: return launch_cta<MERBIT_F32>(c.block, c.ipt, vec, a, s);

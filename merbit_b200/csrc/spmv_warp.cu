@@ -39,6 +39,8 @@
 // per tile serializes at a few ns each, which at ~10^5 tiles per launch
 // costs more than the SpMV itself -- and the look-back cannot deadlock: the
 // smallest unfinished tile has all predecessors finished.
+#include <mutex>
+
 #include "merbit_internal.cuh"
 
 namespace merbit {
@@ -121,7 +123,37 @@ __device__ __forceinline__ void resolve_swap(PendingSwap& p, RS& out) {
     p.row = -1;
 }
 
-template <int DT, int IPT>
+// A row that began two or more tiles before the tile that completes it:
+// its carry-in is the sum of the carries of the tiles in between, which run
+// on other warps at about the same time.  Its look-back is queued and taken
+// later (when the queue is full, else after the warp's last tile), so the
+// warp does not wait for those tiles while it still has tiles to process.
+struct LookBack {
+    double head;  // the completing tile's part of the row
+    int row, u, rs;
+};
+constexpr int kLookBackQueue = 8;
+
+template <class RS>
+__device__ __forceinline__ void drain_look_backs(const SpmvLaunch& a, unsigned epoch,
+                                                 const LookBack* q, int n, int lane, RS& out) {
+    for (int i = 0; i < n; ++i) {
+        const LookBack e = q[i];
+        const double total = look_back(a.coords, a.slots, a.nslots, epoch, a.state, e.u, e.rs, lane);
+        if (lane == 0) out(e.row, total + e.head);
+    }
+    __syncwarp();
+}
+
+// x gather: through L1 (ld.global.nc), or, CG, cached in L2 only (no L1
+// line is allocated, which leaves L1 to other gathers in flight; better when
+// x has no reuse within an SM).
+template <bool CG, typename T>
+__device__ __forceinline__ T gather_x(const T* p) {
+    return CG ? __ldcg(p) : __ldg(p);
+}
+
+template <int DT, int IPT, bool CG = false>
 struct WarpTile {
     using Pr = Prec<DT>;
     using V = typename Pr::V;
@@ -164,7 +196,8 @@ struct WarpTile {
     template <class RS>
     static __device__ __forceinline__ void process(const SpmvLaunch& a, int u, unsigned epoch,
                                                    unsigned char* ws, int lane,
-                                                   PendingSwap& pa, PendingSwap& pb, RS& out) {
+                                                   PendingSwap& pa, PendingSwap& pb, RS& out,
+                                                   LookBack* lbq, int& nlb) {
         const int* s_rp = reinterpret_cast<const int*>(ws);
         const int* s_col = reinterpret_cast<const int*>(ws + S::rp_bytes);
         const V* s_val = reinterpret_cast<const V*>(ws + S::rp_bytes + S::col_bytes);
@@ -188,7 +221,7 @@ struct WarpTile {
 #pragma unroll
             for (int j = 0; j < IPT; ++j) {
                 const int i = lane + 32 * j;
-                xg[j] = i < nz ? __ldg(xv + s_col[x0 + i - col_base]) : (X)0;
+                xg[j] = i < nz ? gather_x<CG>(xv + s_col[x0 + i - col_base]) : (X)0;
             }
             Acc acc;
             acc.zero();
@@ -239,7 +272,7 @@ struct WarpTile {
 #pragma unroll
             for (int j = 0; j < IPT; ++j) {
                 const int i = lane + 32 * j;
-                xg[j] = i < nz ? __ldg(xv + cidx[j]) : (X)0;
+                xg[j] = i < nz ? gather_x<CG>(xv + cidx[j]) : (X)0;
             }
 #pragma unroll
             for (int j = 0; j < IPT; ++j) {
@@ -355,20 +388,32 @@ struct WarpTile {
                     pb.carry = 0;
                 }
             } else {
-                const double total =
-                    look_back(a.coords, a.slots, a.nslots, epoch, a.state, u, rs, lane);
-                if (holds_first) out(y0, total + rv);
+                if (nlb == kLookBackQueue) {  // warp-uniform
+                    drain_look_backs(a, epoch, lbq, nlb, lane, out);
+                    nlb = 0;
+                }
+                if (holds_first) {
+                    LookBack e;
+                    e.head = rv;
+                    e.row = y0;
+                    e.u = u;
+                    e.rs = rs;
+                    lbq[nlb] = e;
+                }
+                ++nlb;
+                __syncwarp();
             }
         }
     }
 };
 
-template <int DT, int WARPS, int IPT, int STAGES, bool RES>
+template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG>
 __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch a) {
-    using T = WarpTile<DT, IPT>;
+    using T = WarpTile<DT, IPT, CG>;
     using S = typename T::S;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned s_epoch;
+    __shared__ LookBack s_lbq[WARPS][kLookBackQueue];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_epoch = *(volatile unsigned*)&a.state->epoch;
@@ -388,6 +433,7 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch 
     const int nw = (int)gridDim.x * WARPS;
     unsigned phases = 0u;
     RowStore<typename T::Y, RES> out(a);
+    int nlb = 0;  // queued look-backs of this warp
     PendingSwap pa, pb;
     pa.row = pb.row = -1;
     pa.got = pb.got = kEmpty;
@@ -410,7 +456,7 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch 
             __all_sync(0xFFFFFFFFu, mbar_wait_bounded(cbar, (phases >> k) & 1u, a.state));
         phases ^= 1u << k;
         __syncwarp();
-        if (ok) T::process(a, u, epoch, cur, lane, pa, pb, out);
+        if (ok) T::process(a, u, epoch, cur, lane, pa, pb, out, s_lbq[warp], nlb);
         if (STAGES == 1) {
             if (un < a.num_tiles) T::issue(a, un, cur, cbar, lane);
         } else {
@@ -419,6 +465,7 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch 
     }
     resolve_swap(pa, out);
     resolve_swap(pb, out);
+    drain_look_backs(a, epoch, s_lbq[warp], nlb, lane, out);
     if (RES) {
         finish_launch_residual<WARPS>(a.state, epoch, out.res, a.partials, (int)blockIdx.x,
                                       (int)gridDim.x, a.residual);
@@ -429,72 +476,107 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch 
 }
 
 namespace {
-template <int DT, int WARPS, int IPT, int STAGES, bool RES>
-int launch_warp_k(const SpmvLaunch& a, cudaStream_t s) {
-    using S = WarpSmem<typename Prec<DT>::V, typename Prec<DT>::P, IPT>;
-    constexpr size_t smem = S::bytes * WARPS * STAGES;
-    static int grid_cap[64] = {};  // resident CTAs per device, from the occupancy calculator
-    if (RES && !a.partials) return fail(MERBIT_ERR_INVALID, "spmv_warp: residual without partials");
+// Launches a persistent cooperative grid of `kern` (all CTAs resident).
+// `carveout` (percent of the largest shared-memory size, 0 = the driver's
+// choice) goes with the launch as its preferred shared-memory / L1 split.
+// The grid is the occupancy under that split, computed once per device and
+// split: the occupancy calculator reads the function's preferred carveout,
+// so it is set for the query and put back to "no preference" afterwards
+// (every launch that wants a split passes it as a launch attribute).
+template <typename K>
+int launch_coop(K kern, int warps, size_t smem, int carveout, int (*grid_cap)[3],
+                const SpmvLaunch& a, cudaStream_t s, const char* name) {
+    static std::mutex mu;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmv_warp: device ordinal >= 64");
-    auto kern = spmv_warp_kernel<DT, WARPS, IPT, STAGES, RES>;
-    if (grid_cap[dev] == 0) {
+    const int slot = carveout == 0 ? 0 : (carveout == kCarveoutL1 ? 1 : 2);
+    if (slot == 2 && carveout != kCarveoutL1Max)
+        return fail(MERBIT_ERR_INVALID, "spmv_warp: unsupported carveout");
+    int cap = __atomic_load_n(&grid_cap[dev][slot], __ATOMIC_ACQUIRE);
+    if (cap == 0) {
+        std::lock_guard<std::mutex> lk(mu);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(spmv_warp)");
+        if (e != cudaSuccess) return cuda_fail(e, name);
+        if (carveout) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
+            if (e != cudaSuccess) return cuda_fail(e, name);
+        }
         int per_sm = 0, sms = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem);
-        if (e != cudaSuccess) return cuda_fail(e, "occupancy(spmv_warp)");
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
+        if (carveout) {
+            const cudaError_t e2 = cudaFuncSetAttribute(
+                kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutDefault);
+            if (e == cudaSuccess) e = e2;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, name);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        grid_cap[dev] = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
+        cap = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
+        __atomic_store_n(&grid_cap[dev][slot], cap, __ATOMIC_RELEASE);
     }
-    const long long need = ((long long)a.num_tiles + WARPS - 1) / WARPS;
-    const int grid = (int)(need < grid_cap[dev] ? need : grid_cap[dev]);
+    const long long need = ((long long)a.num_tiles + warps - 1) / warps;
+    const int grid = (int)(need < cap ? need : cap);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3(WARPS * 32);
+    cfg.blockDim = dim3(warps * 32);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (carveout) {
+        attr[1].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+        attr[1].val.sharedMemCarveout = (unsigned)carveout;
+        cfg.numAttrs = 2;
+    }
+    cfg.attrs = attr;
     cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
     if (e == cudaSuccess) e = cudaGetLastError();
-    return e == cudaSuccess ? (int)MERBIT_OK : cuda_fail(e, "spmv_warp_kernel launch");
+    return e == cudaSuccess ? (int)MERBIT_OK : cuda_fail(e, name);
 }
 
-template <int DT, int WARPS, int IPT, int STAGES>
-int launch_warp(const SpmvLaunch& a, cudaStream_t s) {
-    return a.residual ? launch_warp_k<DT, WARPS, IPT, STAGES, true>(a, s)
-                      : launch_warp_k<DT, WARPS, IPT, STAGES, false>(a, s);
+template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG>
+int launch_warp_k(const SpmvLaunch& a, int carveout, cudaStream_t s) {
+    using S = typename WarpTile<DT, IPT, CG>::S;
+    static int grid_cap[64][3] = {};
+    if (RES && !a.partials) return fail(MERBIT_ERR_INVALID, "spmv_warp: residual without partials");
+    return launch_coop(spmv_warp_kernel<DT, WARPS, IPT, STAGES, RES, CG>, WARPS,
+                       S::bytes * WARPS * STAGES, carveout, grid_cap, a, s, "spmv_warp_kernel");
+}
+
+template <int DT, int WARPS, int IPT, int STAGES, bool CG>
+int launch_warp(const SpmvLaunch& a, int carveout, cudaStream_t s) {
+    return a.residual ? launch_warp_k<DT, WARPS, IPT, STAGES, true, CG>(a, carveout, s)
+                      : launch_warp_k<DT, WARPS, IPT, STAGES, false, CG>(a, carveout, s);
 }
 
 template <int DT>
-int launch_warp_dt(int warps, int ipt, int stages, const SpmvLaunch& a, cudaStream_t s) {
-    if (stages == 2) {
-        if (warps == 4 && ipt == 15) return launch_warp<DT, 4, 15, 2>(a, s);
-        if (warps == 4 && ipt == 7) return launch_warp<DT, 4, 7, 2>(a, s);
+int launch_warp_dt(const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s) {
+    const int warps = c.block / 32, ipt = c.ipt;
+    if (c.stages != 1) return fail(MERBIT_ERR_INVALID, "spmv_warp: no such configuration");
+    if (c.cg) {
+        if (warps == 8 && ipt == 15) return launch_warp<DT, 8, 15, 1, true>(a, c.carveout, s);
+        if (warps == 4 && ipt == 15) return launch_warp<DT, 4, 15, 1, true>(a, c.carveout, s);
+        if (warps == 8 && ipt == 11) return launch_warp<DT, 8, 11, 1, true>(a, c.carveout, s);
     } else {
-        if (warps == 4 && ipt == 15) return launch_warp<DT, 4, 15, 1>(a, s);
-        if (warps == 8 && ipt == 15) return launch_warp<DT, 8, 15, 1>(a, s);
-        if (warps == 8 && ipt == 11) return launch_warp<DT, 8, 11, 1>(a, s);
-        if (warps == 4 && ipt == 23) return launch_warp<DT, 4, 23, 1>(a, s);
-        if (warps == 8 && ipt == 7) return launch_warp<DT, 8, 7, 1>(a, s);
+        if (warps == 8 && ipt == 15) return launch_warp<DT, 8, 15, 1, false>(a, c.carveout, s);
+        if (warps == 4 && ipt == 15) return launch_warp<DT, 4, 15, 1, false>(a, c.carveout, s);
+        if (warps == 8 && ipt == 11) return launch_warp<DT, 8, 11, 1, false>(a, c.carveout, s);
+        if (warps == 4 && ipt == 23) return launch_warp<DT, 4, 23, 1, false>(a, c.carveout, s);
+        if (warps == 8 && ipt == 7) return launch_warp<DT, 8, 7, 1, false>(a, c.carveout, s);
     }
     return fail(MERBIT_ERR_INVALID, "spmv_warp: no such configuration");
 }
 }  // namespace
 
-int spmv_warp_launch(int dtype, int warps, int ipt, int stages, const SpmvLaunch& a,
-                     cudaStream_t s) {
+int spmv_warp_launch(int dtype, const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s) {
     if (a.num_tiles <= 0) return MERBIT_OK;
     switch (dtype) {
-    case MERBIT_F64: return launch_warp_dt<MERBIT_F64>(warps, ipt, stages, a, s);
-    case MERBIT_F32: return launch_warp_dt<MERBIT_F32>(warps, ipt, stages, a, s);
-    case MERBIT_BF16: return launch_warp_dt<MERBIT_BF16>(warps, ipt, stages, a, s);
+    case MERBIT_F64: return launch_warp_dt<MERBIT_F64>(c, a, s);
+    case MERBIT_F32: return launch_warp_dt<MERBIT_F32>(c, a, s);
+    case MERBIT_BF16: return launch_warp_dt<MERBIT_BF16>(c, a, s);
     }
     return fail(MERBIT_ERR_INVALID, "spmv_warp: bad dtype");
 }
