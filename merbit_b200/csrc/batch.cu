@@ -70,7 +70,11 @@ SpmmDesc make_desc(merbit_plan_s* p, const Partition* part, const void* x, long 
 // One launch over columns [0, kk) of X / Y (pointers already offset).
 int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long ldx, double beta,
                void* y, long long ldy, cudaStream_t s) {
-    const int items = kDefaultItems;
+    // the 512-item tiles (vector width 4) measured faster for k >= 4 on the
+    // power-law and banded matrices; other shapes keep 256
+    const int esz = (int)xy_size(p->dtype);
+    int items = kDefaultItems;
+    if (kk >= 4 && pick_vw(kk, ldx, x, y, ldy, esz, 512) == 4) items = 512;
     const Partition* part = nullptr;
     int st = plan_partition(p, items, &part, s);
     if (st != MERBIT_OK) return st;
@@ -82,7 +86,6 @@ int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long 
         if (st != MERBIT_OK) return st;
         it = p->spmm_slots.emplace(key, sl).first;
     }
-    const int esz = (int)xy_size(p->dtype);
     const int vw = pick_vw(kk, ldx, x, y, ldy, esz, items);
     SpmmLaunch a = {};
     a.single = make_desc(p, part, x, ldx, y, ldy, 0);

@@ -67,54 +67,148 @@ int grid_for(long long n) {
     return (int)(g > 0 ? g : 1);
 }
 
-// dval: groups of LPG lanes per nonzero, VW values per lane.
-template <typename Xt, int LPG, int VW>
-__global__ void dval_kernel(const int32_t* __restrict__ col, const int* __restrict__ row_of,
-                            int nnz, int k, const Xt* __restrict__ g, long long ldg,
-                            const Xt* __restrict__ x, long long ldx, Xt* __restrict__ out) {
+// dval[e] = G[row_e] . X[col_e].  Groups of LPG lanes take one nonzero, each
+// lane VW consecutive RHS values per vector load (k = LPG * VW * n); a warp
+// takes U * (32 / LPG) nonzeros per step and issues all their loads before
+// it uses any, so each lane keeps 2U vector loads in flight.  Products of
+// the stored values are exact in double and summed in a fixed order (lane
+// sums, then a butterfly over the group).
+template <typename Xt, int VW>
+struct DvalVec;
+template <>
+struct DvalVec<float, 4> {
+    static __device__ __forceinline__ void ld(const float* p, float (&o)[4]) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+        o[2] = t.z;
+        o[3] = t.w;
+    }
+};
+template <>
+struct DvalVec<float, 2> {
+    static __device__ __forceinline__ void ld(const float* p, float (&o)[2]) {
+        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+    }
+};
+template <>
+struct DvalVec<double, 2> {
+    static __device__ __forceinline__ void ld(const double* p, double (&o)[2]) {
+        const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+    }
+};
+template <typename Xt>
+struct DvalVec<Xt, 1> {
+    static __device__ __forceinline__ void ld(const Xt* p, Xt (&o)[1]) { o[0] = __ldg(p); }
+};
+
+template <typename Xt, int LPG, int VW, int U>
+__global__ void __launch_bounds__(256) dval_kernel(const int32_t* __restrict__ col,
+                                                   const int* __restrict__ row_of, int nnz, int k,
+                                                   const Xt* __restrict__ g, long long ldg,
+                                                   const Xt* __restrict__ x, long long ldx,
+                                                   Xt* __restrict__ out) {
+    constexpr int GPW = 32 / LPG;
     const int lane = threadIdx.x & 31;
     const int grp = lane / LPG, jl = lane % LPG;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    constexpr int GPW = 32 / LPG;
-    for (long long base = gw * GPW; base < nnz; base += nwarps * GPW) {
-        const long long e = base + grp;
-        double acc = 0.0;
-        if (e < nnz) {
-            const int r = __ldg(row_of + e), c = __ldg(col + e);
-            for (int j = jl * VW; j < k; j += LPG * VW) {
+    for (long long base = gw * (U * GPW); base < nnz; base += nwarps * (U * GPW)) {
+        int r[U], c[U];
 #pragma unroll
-                for (int v = 0; v < VW; ++v)
-                    if (j + v < k)
-                        acc += (double)__ldg(g + (size_t)r * ldg + j + v) *
-                               (double)__ldg(x + (size_t)c * ldx + j + v);
+        for (int u = 0; u < U; ++u) {
+            const long long e = base + u * GPW + grp;
+            r[u] = e < nnz ? __ldg(row_of + e) : -1;
+            c[u] = e < nnz ? __ldg(col + e) : 0;
+        }
+        double acc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc[u] = 0.0;
+        for (int j = jl * VW; j < k; j += LPG * VW) {
+            Xt gv[U][VW], xv[U][VW];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (r[u] >= 0) {
+                    DvalVec<Xt, VW>::ld(g + (size_t)r[u] * ldg + j, gv[u]);
+                    DvalVec<Xt, VW>::ld(x + (size_t)c[u] * ldx + j, xv[u]);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < VW; ++v) gv[u][v] = xv[u][v] = (Xt)0;
+                }
             }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int v = 0; v < VW; ++v) acc[u] = fma((double)gv[u][v], (double)xv[u][v], acc[u]);
         }
 #pragma unroll
-        for (int o = LPG / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-        if (e < nnz && jl == 0) out[e] = (Xt)acc;
+        for (int o = LPG / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc[u] += __shfl_xor_sync(0xFFFFFFFFu, acc[u], o);
+        if (jl == 0) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const long long e = base + u * GPW + grp;
+                if (e < nnz) out[e] = (Xt)acc[u];
+            }
+        }
     }
+}
+
+// Widest VW the leading dimensions and base pointers allow for this k.
+template <typename Xt>
+int dval_vw(int k, long long ldg, long long ldx, const void* g, const void* x) {
+    const int vmax = sizeof(Xt) == 4 ? 4 : 2;
+    for (int vw = vmax; vw > 1; vw >>= 1) {
+        const size_t a = (size_t)vw * sizeof(Xt);
+        if (k % vw == 0 && ldg % vw == 0 && ldx % vw == 0 && (uintptr_t)g % a == 0 &&
+            (uintptr_t)x % a == 0)
+            return vw;
+    }
+    return 1;
+}
+
+template <typename Xt, int VW>
+int launch_dval_vw(int k, int nnz, const int32_t* col, const int* row_of, const Xt* g,
+                   long long ldg, const Xt* x, long long ldx, Xt* out, cudaStream_t s) {
+    // lanes per nonzero: enough to cover k in one pass when k <= 32*VW
+    const int per = (k + VW - 1) / VW;
+    const int grid = 148 * 8;
+#define MERBIT_DVAL(L)                                                                     \
+    dval_kernel<Xt, L, VW, 4><<<grid, 256, 0, s>>>(col, row_of, nnz, k, g, ldg, x, ldx, out)
+    if (per <= 1)
+        MERBIT_DVAL(1);
+    else if (per <= 2)
+        MERBIT_DVAL(2);
+    else if (per <= 4)
+        MERBIT_DVAL(4);
+    else if (per <= 8)
+        MERBIT_DVAL(8);
+    else if (per <= 16)
+        MERBIT_DVAL(16);
+    else
+        MERBIT_DVAL(32);
+#undef MERBIT_DVAL
+    MERBIT_CUDA(cudaGetLastError());
+    return MERBIT_OK;
 }
 
 template <typename Xt>
 int launch_dval(const merbit_plan_s* p, int k, const void* g, long long ldg, const void* x,
                 long long ldx, void* out, cudaStream_t s) {
-    const int grid = grid_for((long long)p->nnz * 4);
     const Xt* gg = static_cast<const Xt*>(g);
     const Xt* xx = static_cast<const Xt*>(x);
     Xt* oo = static_cast<Xt*>(out);
-    if (k >= 32)
-        dval_kernel<Xt, 32, 1><<<grid, 256, 0, s>>>(p->col, p->row_of, p->nnz, k, gg, ldg, xx, ldx, oo);
-    else if (k >= 16)
-        dval_kernel<Xt, 16, 1><<<grid, 256, 0, s>>>(p->col, p->row_of, p->nnz, k, gg, ldg, xx, ldx, oo);
-    else if (k >= 8)
-        dval_kernel<Xt, 8, 1><<<grid, 256, 0, s>>>(p->col, p->row_of, p->nnz, k, gg, ldg, xx, ldx, oo);
-    else if (k >= 4)
-        dval_kernel<Xt, 4, 1><<<grid, 256, 0, s>>>(p->col, p->row_of, p->nnz, k, gg, ldg, xx, ldx, oo);
-    else
-        dval_kernel<Xt, 1, 1><<<grid, 256, 0, s>>>(p->col, p->row_of, p->nnz, k, gg, ldg, xx, ldx, oo);
-    MERBIT_CUDA(cudaGetLastError());
-    return MERBIT_OK;
+    const int vw = dval_vw<Xt>(k, ldg, ldx, g, x);
+    if constexpr (sizeof(Xt) == 4) {
+        if (vw == 4) return launch_dval_vw<Xt, 4>(k, p->nnz, p->col, p->row_of, gg, ldg, xx, ldx, oo, s);
+    }
+    if (vw == 2) return launch_dval_vw<Xt, 2>(k, p->nnz, p->col, p->row_of, gg, ldg, xx, ldx, oo, s);
+    return launch_dval_vw<Xt, 1>(k, p->nnz, p->col, p->row_of, gg, ldg, xx, ldx, oo, s);
 }
 
 int ensure_row_of(merbit_plan_s* p, cudaStream_t s) {

@@ -124,3 +124,29 @@ def test_backward_deterministic_and_refresh():
         v.mul_(2.0)
     d3 = M.transpose_plan(v).spmm(G)
     assert torch.allclose(d3, 2 * d1, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("k,ld", [(1, 1), (2, 3), (3, 3), (8, 12), (16, 17), (32, 32), (40, 44)])
+def test_dval_strided_operands(dtype, k, ld):
+    """dval with leading dimensions larger than k (vector widths 1, 2 and 4
+    are chosen from the alignment) against the oracle."""
+    A = synth.workload("zipf_2k_diff")
+    nt = np.float64 if dtype == "f64" else np.float32
+    tt = torch.float64 if dtype == "f64" else torch.float32
+    Xw = torch.from_numpy(synth.uniform(7, A.ncol * ld).reshape(A.ncol, ld).astype(nt)).cuda()
+    Gw = torch.from_numpy(synth.normal(8, A.nrow * ld).reshape(A.nrow, ld).astype(nt)).cuda()
+    X, G = Xw[:, :k], Gw[:, :k]
+    rp, col, v = to_cuda(A, dtype)
+    M = SparseMatrix(rp, col, v)
+    out = torch.empty(A.nnz, dtype=tt, device="cuda")
+    from merbit_b200 import _check, _dptr, _stream_ptr, lib
+
+    _check(lib().merbit_dval(M.plan._h, k, _dptr(G), ld, _dptr(X), ld, _dptr(out),
+                             _stream_ptr(None)))
+    Gh, Xh = G.cpu().numpy(), X.cpu().numpy()
+    ref = O.dval(A.row_ptr, A.col, np.ascontiguousarray(Gh), np.ascontiguousarray(Xh))
+    den = O.dval(A.row_ptr, A.col, np.abs(Gh).astype(np.float64), np.abs(Xh).astype(np.float64))
+    tol = 1e-13 if dtype == "f64" else 1e-6
+    assert (np.abs(out.cpu().numpy() - ref) / np.maximum(den, 1e-300)).max() <= tol
