@@ -407,7 +407,9 @@ struct WarpTile {
     }
 };
 
-template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG>
+// CV: the shared-memory carveout the kernel is launched with (it does not
+// change the code; each split gets its own function and function attribute).
+template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG, int CV>
 __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch a) {
     using T = WarpTile<DT, IPT, CG>;
     using S = typename T::S;
@@ -478,22 +480,18 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch 
 namespace {
 // Launches a persistent cooperative grid of `kern` (all CTAs resident).
 // `carveout` (percent of the largest shared-memory size, 0 = the driver's
-// choice) goes with the launch as its preferred shared-memory / L1 split.
-// The grid is the occupancy under that split, computed once per device and
-// split: the occupancy calculator reads the function's preferred carveout,
-// so it is set for the query and put back to "no preference" afterwards
-// (every launch that wants a split passes it as a launch attribute).
+// choice) is the kernel's preferred shared-memory / L1 split: every kernel
+// instantiation has one fixed split (a template parameter), set once as the
+// function's attribute before the occupancy query that sizes the grid, and
+// passed again with each launch.
 template <typename K>
-int launch_coop(K kern, int warps, size_t smem, int carveout, int (*grid_cap)[3],
-                const SpmvLaunch& a, cudaStream_t s, const char* name) {
+int launch_coop(K kern, int warps, size_t smem, int carveout, int* grid_cap, const SpmvLaunch& a,
+                cudaStream_t s, const char* name) {
     static std::mutex mu;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmv_warp: device ordinal >= 64");
-    const int slot = carveout == 0 ? 0 : (carveout == kCarveoutL1 ? 1 : 2);
-    if (slot == 2 && carveout != kCarveoutL1Max)
-        return fail(MERBIT_ERR_INVALID, "spmv_warp: unsupported carveout");
-    int cap = __atomic_load_n(&grid_cap[dev][slot], __ATOMIC_ACQUIRE);
+    int cap = __atomic_load_n(&grid_cap[dev], __ATOMIC_ACQUIRE);
     if (cap == 0) {
         std::lock_guard<std::mutex> lk(mu);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -505,15 +503,10 @@ int launch_coop(K kern, int warps, size_t smem, int carveout, int (*grid_cap)[3]
         }
         int per_sm = 0, sms = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
-        if (carveout) {
-            const cudaError_t e2 = cudaFuncSetAttribute(
-                kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutDefault);
-            if (e == cudaSuccess) e = e2;
-        }
         if (e != cudaSuccess) return cuda_fail(e, name);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cap = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
-        __atomic_store_n(&grid_cap[dev][slot], cap, __ATOMIC_RELEASE);
+        __atomic_store_n(&grid_cap[dev], cap, __ATOMIC_RELEASE);
     }
     const long long need = ((long long)a.num_tiles + warps - 1) / warps;
     const int grid = (int)(need < cap ? need : cap);
@@ -537,36 +530,41 @@ int launch_coop(K kern, int warps, size_t smem, int carveout, int (*grid_cap)[3]
     return e == cudaSuccess ? (int)MERBIT_OK : cuda_fail(e, name);
 }
 
-template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG>
-int launch_warp_k(const SpmvLaunch& a, int carveout, cudaStream_t s) {
+template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG, int CV>
+int launch_warp_k(const SpmvLaunch& a, cudaStream_t s) {
     using S = typename WarpTile<DT, IPT, CG>::S;
-    static int grid_cap[64][3] = {};
+    static int grid_cap[64] = {};
     if (RES && !a.partials) return fail(MERBIT_ERR_INVALID, "spmv_warp: residual without partials");
-    return launch_coop(spmv_warp_kernel<DT, WARPS, IPT, STAGES, RES, CG>, WARPS,
-                       S::bytes * WARPS * STAGES, carveout, grid_cap, a, s, "spmv_warp_kernel");
+    return launch_coop(spmv_warp_kernel<DT, WARPS, IPT, STAGES, RES, CG, CV>, WARPS,
+                       S::bytes * WARPS * STAGES, CV, grid_cap, a, s, "spmv_warp_kernel");
 }
 
-template <int DT, int WARPS, int IPT, int STAGES, bool CG>
-int launch_warp(const SpmvLaunch& a, int carveout, cudaStream_t s) {
-    return a.residual ? launch_warp_k<DT, WARPS, IPT, STAGES, true, CG>(a, carveout, s)
-                      : launch_warp_k<DT, WARPS, IPT, STAGES, false, CG>(a, carveout, s);
+template <int DT, int WARPS, int IPT, int STAGES, bool CG, int CV>
+int launch_warp(const SpmvLaunch& a, cudaStream_t s) {
+    return a.residual ? launch_warp_k<DT, WARPS, IPT, STAGES, true, CG, CV>(a, s)
+                      : launch_warp_k<DT, WARPS, IPT, STAGES, false, CG, CV>(a, s);
 }
 
+// The (warps, items per thread, gather hint, carveout) combinations of the
+// configuration tables in spmv.cu.
 template <int DT>
 int launch_warp_dt(const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s) {
     const int warps = c.block / 32, ipt = c.ipt;
     if (c.stages != 1) return fail(MERBIT_ERR_INVALID, "spmv_warp: no such configuration");
-    if (c.cg) {
-        if (warps == 8 && ipt == 15) return launch_warp<DT, 8, 15, 1, true>(a, c.carveout, s);
-        if (warps == 4 && ipt == 15) return launch_warp<DT, 4, 15, 1, true>(a, c.carveout, s);
-        if (warps == 8 && ipt == 11) return launch_warp<DT, 8, 11, 1, true>(a, c.carveout, s);
-    } else {
-        if (warps == 8 && ipt == 15) return launch_warp<DT, 8, 15, 1, false>(a, c.carveout, s);
-        if (warps == 4 && ipt == 15) return launch_warp<DT, 4, 15, 1, false>(a, c.carveout, s);
-        if (warps == 8 && ipt == 11) return launch_warp<DT, 8, 11, 1, false>(a, c.carveout, s);
-        if (warps == 4 && ipt == 23) return launch_warp<DT, 4, 23, 1, false>(a, c.carveout, s);
-        if (warps == 8 && ipt == 7) return launch_warp<DT, 8, 7, 1, false>(a, c.carveout, s);
-    }
+#define MERBIT_WARP_CASE(W, I, G, C)                                                   \
+    if (warps == W && ipt == I && c.cg == G && c.carveout == C)                        \
+        return launch_warp<DT, W, I, 1, G, C>(a, s);
+    MERBIT_WARP_CASE(8, 15, 1, kCarveoutL1)
+    MERBIT_WARP_CASE(4, 15, 1, kCarveoutL1)
+    MERBIT_WARP_CASE(8, 11, 1, kCarveoutL1)
+    MERBIT_WARP_CASE(4, 15, 1, kCarveoutL1Max)
+    MERBIT_WARP_CASE(8, 15, 0, kCarveoutL1)
+    MERBIT_WARP_CASE(8, 15, 0, 0)
+    MERBIT_WARP_CASE(4, 15, 0, 0)
+    MERBIT_WARP_CASE(8, 11, 0, 0)
+    MERBIT_WARP_CASE(8, 7, 0, 0)
+    MERBIT_WARP_CASE(4, 23, 0, 0)
+#undef MERBIT_WARP_CASE
     return fail(MERBIT_ERR_INVALID, "spmv_warp: no such configuration");
 }
 }  // namespace
