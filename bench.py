@@ -233,6 +233,44 @@ def cpu_baseline(A, x, seconds: float):
     return y, med, threads, len(times)
 
 
+def gather_ceiling(A, dev, stream, reps: int = 10):
+    """Random-gather rate of this GPU (G gathers/s): a pure gather loop over
+    nnz uniformly random columns of a double vector of ncol entries."""
+    import ctypes as C
+
+    import torch
+
+    import merbit_b200 as mb
+
+    n = A.nnz - A.nnz % 16
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    idx = torch.randint(0, A.ncol, (n,), dtype=torch.int32, device=dev, generator=g)
+    xg = torch.rand(A.ncol, dtype=torch.float64, device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    out = torch.empty(sms * 2048, dtype=torch.float64, device=dev)
+    L = mb.lib()
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def launch():
+        mb._check(L.merbit_bench_gather(C.c_void_p(xg.data_ptr()), A.ncol,
+                                        C.c_void_p(idx.data_ptr()), n,
+                                        C.c_void_p(out.data_ptr()), out.numel(), sp))
+
+    for _ in range(3):
+        launch()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        launch()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    sec = e0.elapsed_time(e1) / reps * 1e-3
+    del idx, xg, out
+    return n / sec / 1e9
+
+
 def traffic_from_profile(workload: str, dtype: str):
     p = os.path.join(ROOT, "profiles", f"spmv_{dtype}_{workload}_traffic.json")
     if os.path.exists(p):
@@ -300,6 +338,10 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     ms_cold = allreduce_max(ws, statistics.mean(a.elapsed_time(b) for a, b in evs))
     del flush
+
+    # ---- the GPU's random-gather ceiling (merbit_bench_gather): nnz gathers
+    # at uniformly random columns of a double x, 16 in flight per thread
+    gather = gather_ceiling(A, dev, stream)
 
     # ---- e2e through the public API with host buffers
     xh = torch.from_numpy(x).to(xt).pin_memory()
@@ -375,6 +417,14 @@ def run_ours(args):
             "peak_source": f"{peak_src} hbm_gbs (copy), burst",
             "traffic": traffic,
             "kernel": KERNEL_OF_KIND[info.kind],
+            "gather_bound": {
+                "achieved_ggather_s": round(A.nnz / (ms * 1e-3) / 1e9, 1),
+                "ceiling_ggather_s": round(gather, 1),
+                "frac": round(A.nnz / (ms * 1e-3) / 1e9 / gather, 4),
+                "note": "one x gather per nonzero; ceiling = a pure random-gather loop on this "
+                        "GPU (merbit_bench_gather). Binding when columns are random "
+                        "(x misses L1), as for the power-law matrix",
+            },
         },
         "e2e": {
             "value": round(ws * B / (ms_e2e * 1e-3) / 1e9, 2),

@@ -99,6 +99,11 @@ SIGNATURES = {
     "merbit_last_error_detail": (C.c_char_p, []),
 }
 
+# measurement support (include/merbit_bench.h)
+BENCH_SIGNATURES = {
+    "merbit_bench_gather": (C.c_int, [_P, C.c_int32, _P, C.c_int64, _P, C.c_int32, _P]),
+}
+
 _lib = None
 
 
@@ -111,7 +116,7 @@ def lib() -> C.CDLL:
             raise ImportError(
                 f"{LIB_PATH} is missing; build it with `python -m merbit_b200._build`")
         L = C.CDLL(LIB_PATH)
-        for name, (res, args) in SIGNATURES.items():
+        for name, (res, args) in {**SIGNATURES, **BENCH_SIGNATURES}.items():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args

@@ -224,14 +224,18 @@ struct SpmmTile {
                 }
             }
         };
+        // end of row ly (INT_MAX past the segment's last row), kept in a
+        // register so the walk reads row_ptr once per row, not per nonzero
+        int next_end = ly < ly_end ? row_end(s_rp, rpo, ly, x0) : INT_MAX;
         auto consume = [&](int c, const X (&xr)[CH][VW], const V (&vv)[CH]) {
 #pragma unroll
             for (int t = 0; t < CH; ++t) {
                 const int e = c + t;
                 if (e < lx_end) {
-                    while (ly < ly_end && row_end(s_rp, rpo, ly, x0) <= e) {
+                    while (next_end <= e) {
                         emit(ly);
                         ++ly;
+                        next_end = ly < ly_end ? row_end(s_rp, rpo, ly, x0) : INT_MAX;
                     }
                     const P av = to_p(vv[t]);
 #pragma unroll

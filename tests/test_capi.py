@@ -31,6 +31,16 @@ def test_python_binding_covers_header():
     assert set(_declared("merbit.h")) <= set(mb.SIGNATURES)
 
 
+def test_measurement_header_exported_and_bound():
+    L = mb.lib()
+    names = _declared("merbit_bench.h")
+    assert names == ["merbit_bench_gather"]
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) <= set(mb.BENCH_SIGNATURES)
+    assert L.merbit_bench_gather(None, 0, None, 0, None, 0, None) == 1  # MERBIT_ERR_INVALID
+
+
 def test_synth_library_exports():
     from merbit_b200 import synth
 
