@@ -329,43 +329,62 @@ struct SpmmTile {
                     }
                 }
             } else {
-                // fixed-order look-back: steps of 32/K tiles x K columns
-                // (K <= 32), lane l reading column l % K of tile base - l / K
+                // fixed-order look-back over the tiles back to the one that
+                // holds the row start.  Lane l serves column l % K; a step
+                // covers TPS * R tiles (tile offset l / K + TPS * r from
+                // `base`), all loaded before any is summed, so a row spanning
+                // hundreds of tiles takes few dependent round trips.  The
+                // summation order depends only on the tile and the row start.
                 constexpr int TPS = 32 / K > 0 ? 32 / K : 1;
+                constexpr int R = 8;
+                const bool lane_valid = lane < TPS * K;
                 double tot = 0.0;  // column (lane % K) of the sum
                 int base = lt - 1;
                 for (;;) {
-                    const int tq = base - lane / K;
-                    const bool lane_valid = lane < TPS * K;
-                    const bool valid = lane_valid && tq >= 0;
-                    const int cx = valid ? d.coords[tq].x : 0;
-                    const unsigned m = __ballot_sync(0xFFFFFFFFu, lane_valid && (tq < 0 || cx <= rs));
-                    // first tile (lowest lane/K) that holds the row start
-                    const int last_t = m ? (__ffs(m) - 1) / K : TPS - 1;
+                    int tq[R];
+                    int first = INT_MAX;  // smallest offset of a tile starting at or before rs
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const int o = lane / K + TPS * r;
+                        tq[r] = base - o;
+                        if (lane_valid && (tq[r] < 0 || d.coords[tq[r]].x <= rs)) first = min(first, o);
+                    }
+                    first = __reduce_min_sync(0xFFFFFFFFu, first);
+                    unsigned long long bits[R];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const int o = lane / K + TPS * r;
+                        bits[r] = 0ull;  // +0.0
+                        if (lane_valid && tq[r] >= 0 && o <= first)
+                            bits[r] = ld_relaxed_u64(slots + par + (size_t)(d.tile_begin + tq[r]) * K + (lane % K));
+                    }
                     double c = 0.0;
-                    if (valid && lane / K <= last_t) {
-                        const unsigned long long* p =
-                            slots + par + (size_t)(d.tile_begin + tq) * K + (lane % K);
-                        unsigned long long bits = ld_relaxed_u64(p);
-                        if (bits == kEmpty) {
-                            const unsigned long long t0 = global_timer_ns();
-                            while ((bits = ld_relaxed_u64(p)) == kEmpty) {
-                                __nanosleep(32);
-                                if (*(volatile int*)&st->error != 0) break;
-                                if (global_timer_ns() - t0 > kCarryWaitNs) {
-                                    atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
-                                    break;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const int o = lane / K + TPS * r;
+                        if (lane_valid && tq[r] >= 0 && o <= first) {
+                            if (bits[r] == kEmpty) {
+                                const unsigned long long* p =
+                                    slots + par + (size_t)(d.tile_begin + tq[r]) * K + (lane % K);
+                                const unsigned long long t0 = global_timer_ns();
+                                while ((bits[r] = ld_relaxed_u64(p)) == kEmpty) {
+                                    __nanosleep(32);
+                                    if (*(volatile int*)&st->error != 0) break;
+                                    if (global_timer_ns() - t0 > kCarryWaitNs) {
+                                        atomicExch(&st->error, (int)MERBIT_ERR_TIMEOUT);
+                                        break;
+                                    }
                                 }
                             }
+                            c += bits[r] == kEmpty ? 0.0 : __longlong_as_double((long long)bits[r]);
                         }
-                        c = bits == kEmpty ? 0.0 : __longlong_as_double((long long)bits);
                     }
                     // sum over the step's tiles, per column (lanes l, l+K, ...)
 #pragma unroll
                     for (int o = K; o < 32; o <<= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
                     tot += c;
-                    if (m) break;
-                    base -= TPS;
+                    if (first != INT_MAX) break;
+                    base -= TPS * R;
                 }
                 double tv[VW];
 #pragma unroll
