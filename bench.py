@@ -628,9 +628,13 @@ def run_diff(args):
     def fwd():
         M.plan.spmm(X, Y)
 
+    fused = M.backward_fused(G, X) is not None
+
     def bwd():
-        T.spmm(G, dX)
-        M.dval(G, X)
+        # one launch (dX and dval together) where the shape allows it
+        if not fused or M.backward_fused(G, X) is None:
+            T.spmm(G, dX)
+            M.dval(G, X)
 
     for _ in range(max(args.warmup, 3)):
         fwd()
@@ -678,7 +682,9 @@ def run_diff(args):
         "fwd_ms": round(t_f, 4),
         "fwd_bwd_ms": round(t_fb, 4),
         "fwd_bwd_over_fwd": round(t_fb / t_f, 3),
-        "gpu_launches": 3 * n,
+        "gpu_launches": (3 if fused else 4) * n,
+        "backward": "fused transpose SpMM + dval (merbit_spmm_dval)" if fused
+                    else "transpose SpMM, then dval",
         "roofline": {"bound": "hbm", "achieved": round(B / (t_f * 1e-3) / 1e9, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(B / (t_f * 1e-3) / 1e9 / peak, 4),
                      "peak_source": f"{peak_src} hbm_gbs", "traffic": None,

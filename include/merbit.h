@@ -188,6 +188,16 @@ int merbit_plan_transpose_refresh(merbit_plan tplan, const void* d_src_vals, voi
 int merbit_dval(merbit_plan plan, int32_t k, const void* d_g, int64_t ldg, const void* d_x,
                 int64_t ldx, void* d_dval, void* stream);
 
+/* The whole backward of Y = A X in one launch, on the transpose plan tplan
+ * of A (merbit_plan_transpose): dX = A^T G (dX [ncol x lddx], overwritten)
+ * and, from the G rows that product gathers anyway, dval[e] =
+ * sum_{j<k} G[row_e, j] * X[col_e, j] for every nonzero e of A (in A's
+ * nonzero order).  k = 1, 2, 4, 8, 16 or 32; F64 and F32 values.
+ * MERBIT_ERR_UNSUPPORTED otherwise: use merbit_spmm + merbit_dval then.
+ * Sums in a fixed order, no atomics. */
+int merbit_spmm_dval(merbit_plan tplan, int32_t k, const void* d_g, int64_t ldg, const void* d_x,
+                     int64_t ldx, void* d_dx, int64_t lddx, void* d_dval, void* stream);
+
 /* ---------------- k right-hand sides and batches ---------------- */
 
 /* Y[nrow x k] = alpha*A*X[ncol x k] + beta*Y, row-major with leading

@@ -87,6 +87,8 @@ SIGNATURES = {
     "merbit_dval": (C.c_int, [_P, C.c_int32, _P, C.c_int64, _P, C.c_int64, _P, _P]),
     "merbit_spmm": (C.c_int, [_P, C.c_int32, C.c_double, _P, C.c_int64, C.c_double, _P,
                               C.c_int64, _P]),
+    "merbit_spmm_dval": (C.c_int, [_P, C.c_int32, _P, C.c_int64, _P, C.c_int64, _P, C.c_int64,
+                                   _P, _P]),
     "merbit_batch_create": (C.c_int, [_P, C.c_int32, _P, C.c_int32, _P, _P, _P, _P, _P]),
     "merbit_batch_spmm": (C.c_int, [_P, C.c_double, C.c_double, _P]),
     "merbit_batch_tune": (C.c_int, [_P, _P]),

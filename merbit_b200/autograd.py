@@ -5,7 +5,10 @@ Backward:
   dX    = A^T G     merge-path SpMM on the transpose plan
                     (merbit_plan_transpose: stable column sort, so every sum
                     is taken in a fixed order -- no float atomics)
-  dvals = G[row] . X[col]   per nonzero (merbit_dval)
+  dvals = G[row] . X[col]   per nonzero
+When both are needed they come from one launch (merbit_spmm_dval: the
+transpose SpMM forms each dval from the G row it gathers); otherwise, or for
+shapes that launch does not take, merbit_spmm and merbit_dval run apart.
 """
 from __future__ import annotations
 
@@ -61,6 +64,24 @@ class SparseMatrix:
                                  _stream_ptr(None)))
         return out
 
+    def backward_fused(self, G: torch.Tensor, X: torch.Tensor, vals: torch.Tensor | None = None):
+        """(dX, dval) of Y = A X from one launch on the transpose plan, or
+        None when that launch does not take these operands."""
+        k = X.shape[1]
+        if self.plan.dtype == 2 or k not in (1, 2, 4, 8, 16, 32):
+            return None
+        T = self.transpose_plan(vals)
+        dX = torch.empty(self.plan.ncol, k, dtype=self.plan.xy_dtype, device=self.plan.device)
+        dval = torch.empty(self.plan.nnz, dtype=self.plan.xy_dtype, device=self.plan.device)
+        ldg = G.stride(0) if G.shape[0] > 1 else k
+        ldx = X.stride(0) if X.shape[0] > 1 else k
+        st = lib().merbit_spmm_dval(T._h, k, _dptr(G), ldg, _dptr(X), ldx, _dptr(dX), k,
+                                    _dptr(dval), _stream_ptr(None))
+        if st == 6:  # MERBIT_ERR_UNSUPPORTED
+            return None
+        _check(st)
+        return dX, dval
+
     # -- user API -----------------------------------------------------------
     def matmul(self, X: torch.Tensor, vals: torch.Tensor | None = None) -> torch.Tensor:
         vals = self.vals if vals is None else vals
@@ -108,6 +129,11 @@ class _SpMM(torch.autograd.Function):
         mat: SparseMatrix = ctx.mat
         G2 = (G.unsqueeze(1) if ctx.vec else G).contiguous()
         dvals = dX = None
+        if ctx.needs_input_grad[0] and ctx.needs_input_grad[1]:
+            fused = mat.backward_fused(G2, X2, vals)
+            if fused is not None:
+                dX, dv = fused
+                return dv.to(vals.dtype), (dX.squeeze(1) if ctx.vec else dX), None
         if ctx.needs_input_grad[1]:
             dX = mat.transpose_plan(vals).spmm(G2)
             if ctx.vec:

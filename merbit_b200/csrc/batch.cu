@@ -69,12 +69,23 @@ SpmmDesc make_desc(merbit_plan_s* p, const Partition* part, const void* x, long 
 
 // One launch over columns [0, kk) of X / Y (pointers already offset).
 int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long ldx, double beta,
-               void* y, long long ldy, cudaStream_t s) {
+               void* y, long long ldy, cudaStream_t s, const void* dv_x = nullptr,
+               long long dv_ldx = 0, void* dv_out = nullptr) {
+    const int esz = (int)xy_size(p->dtype);
+    // vector width: the widest the operands allow (with a fused dval, dv_x
+    // rows are loaded with the same width)
+    auto width = [&](int items) {
+        int vw = pick_vw(kk, ldx, x, y, ldy, esz, items);
+        if (dv_out)
+            while (vw > 1 && (dv_ldx % vw != 0 || (uintptr_t)dv_x % ((size_t)vw * esz) != 0)) vw >>= 1;
+        return vw;
+    };
     // the 512-item tiles (vector width 4) measured faster for k >= 4 on the
     // power-law and banded matrices; other shapes keep 256
-    const int esz = (int)xy_size(p->dtype);
     int items = kDefaultItems;
-    if (kk >= 4 && pick_vw(kk, ldx, x, y, ldy, esz, 512) == 4) items = 512;
+    if (kk >= 4 && width(512) == 4) items = 512;
+    const int vw = width(items);
+    if (!spmm_config_exists(kk, vw, items)) return MERBIT_ERR_UNSUPPORTED;
     const Partition* part = nullptr;
     int st = plan_partition(p, items, &part, s);
     if (st != MERBIT_OK) return st;
@@ -86,7 +97,6 @@ int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long 
         if (st != MERBIT_OK) return st;
         it = p->spmm_slots.emplace(key, sl).first;
     }
-    const int vw = pick_vw(kk, ldx, x, y, ldy, esz, items);
     SpmmLaunch a = {};
     a.single = make_desc(p, part, x, ldx, y, ldy, 0);
     a.descs = nullptr;
@@ -98,6 +108,12 @@ int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long 
     a.total_tiles = part->num_tiles;
     a.alpha = alpha;
     a.beta = beta;
+    if (dv_out) {
+        a.dv_x = dv_x;
+        a.dv_ldx = dv_ldx;
+        a.dv_perm = p->perm;
+        a.dv_out = dv_out;
+    }
     return spmm_launch(p->dtype, kk, vw, items, a, s);
 }
 
@@ -194,6 +210,26 @@ int merbit_spmm(merbit_plan plan, int32_t k, double alpha, const void* d_x, int6
         j += kk;
     }
     return MERBIT_OK;
+}
+
+int merbit_spmm_dval(merbit_plan tplan, int32_t k, const void* d_g, int64_t ldg, const void* d_x,
+                     int64_t ldx, void* d_dx, int64_t lddx, void* d_dval, void* stream) {
+    if (!tplan) return fail(MERBIT_ERR_INVALID, "spmm_dval: plan is null");
+    if (!tplan->perm) return fail(MERBIT_ERR_INVALID, "spmm_dval: not a transpose plan");
+    if (k < 1 || ldg < k || ldx < k || lddx < k)
+        return fail(MERBIT_ERR_INVALID, "spmm_dval: bad k / leading dimension");
+    if (tplan->dtype == MERBIT_BF16)
+        return fail(MERBIT_ERR_UNSUPPORTED, "spmm_dval: bf16 values (use merbit_spmm + merbit_dval)");
+    if (!pow2(k) || k > 32)
+        return fail(MERBIT_ERR_UNSUPPORTED, "spmm_dval: k must be 1, 2, 4, 8, 16 or 32");
+    if (tplan->nrow == 0) return MERBIT_OK;
+    if (!d_dx || !d_dval || (tplan->ncol > 0 && !d_g) || !d_x)
+        return fail(MERBIT_ERR_INVALID, "spmm_dval: null pointer");
+    const int st = spmm_block(tplan, k, 1.0, d_g, ldg, 0.0, d_dx, lddx, (cudaStream_t)stream, d_x,
+                              ldx, d_dval);
+    if (st == MERBIT_ERR_UNSUPPORTED)
+        return fail(MERBIT_ERR_UNSUPPORTED, "spmm_dval: no configuration for these operands");
+    return st;
 }
 
 int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* plans, int32_t k,

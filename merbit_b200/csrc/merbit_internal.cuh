@@ -507,6 +507,13 @@ struct SpmmLaunch {
     LaunchState* state;
     int total_tiles;
     double alpha, beta;
+    // Fused dL/dval (single matrix that is a transpose plan): for every
+    // nonzero e of this matrix, dv_out[dv_perm[e]] = sum over the launch's
+    // columns j of dv_x[row(e), j] * x[col(e), j].  NULL: not fused.
+    const void* dv_x = nullptr;
+    long long dv_ldx = 0;
+    const int* dv_perm = nullptr;
+    void* dv_out = nullptr;
 };
 
 // Launches the SpMM kernel for k right-hand sides, vw values per lane and

@@ -78,7 +78,9 @@ __device__ __forceinline__ unsigned long long dbits(double v) {
 
 }  // namespace
 
-template <int DT, int K, int VW, int ITEMS>
+// DV: also form dL/dval for each nonzero (SpmmLaunch::dv_*), from the x row
+// the walk gathers anyway and the current row of dv_x.
+template <int DT, int K, int VW, int ITEMS, bool DV = false>
 struct SpmmTile {
     using Pr = Prec<DT>;
     using V = typename Pr::V;
@@ -95,14 +97,18 @@ struct SpmmTile {
     static constexpr size_t rp_bytes = a16((size_t)RPC * 4);
     static constexpr size_t col_bytes = a16((size_t)CAP * 4);
     static constexpr size_t val_bytes = a16((size_t)CAP * sizeof(V));
-    static constexpr size_t bar_offset = rp_bytes + col_bytes + val_bytes;
+    // DV: the tile's slice of the transpose permutation, staged like col
+    static constexpr size_t perm_bytes = DV ? a16((size_t)CAP * 4) : 0;
+    static constexpr size_t perm_offset = rp_bytes + col_bytes + val_bytes;
+    static constexpr size_t bar_offset = perm_offset + perm_bytes;
     static constexpr size_t bytes = bar_offset + 16;
     static constexpr int GV = 16 / (int)sizeof(V);
     static_assert(LPG >= 1 && LPG <= 32 && 32 % LPG == 0, "K/VW must divide 32");
     static_assert(SEG * G == ITEMS, "ITEMS must be a multiple of the group count");
 
     static __device__ __forceinline__ void issue(const SpmmDesc& d, int lt, unsigned char* ws,
-                                                 uint64_t* bar, int lane) {
+                                                 uint64_t* bar, int lane,
+                                                 const int* perm = nullptr) {
         const int2 c0 = d.coords[lt];
         const int2 c1 = d.coords[lt + 1];
         int* s_rp = reinterpret_cast<int*>(ws);
@@ -117,7 +123,8 @@ struct SpmmTile {
             return b_end > base ? (unsigned)(b_end - base) * (unsigned)esz : 0u;
         };
         const unsigned tot = bb(c0.y, c1.y + 1, nrp, 4, 4) + bb(c0.x, c1.x, d.nnz, 4, 4) +
-                             bb(c0.x, c1.x, d.nnz, GV, (int)sizeof(V));
+                             bb(c0.x, c1.x, d.nnz, GV, (int)sizeof(V)) +
+                             (DV ? bb(c0.x, c1.x, d.nnz, 4, 4) : 0u);
         __syncwarp();
         if (lane == 0) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -138,6 +145,7 @@ struct SpmmTile {
         stage(s_rp, d.row_ptr, c0.y, c1.y + 1, nrp);
         stage(s_col, d.col, c0.x, c1.x, d.nnz);
         stage(s_val, vals, c0.x, c1.x, d.nnz);
+        if (DV) stage(reinterpret_cast<int*>(ws + perm_offset), perm, c0.x, c1.x, d.nnz);
     }
 
     // Row ends of the tile as nonzero positions relative to x0.
@@ -227,6 +235,13 @@ struct SpmmTile {
         // end of row ly (INT_MAX past the segment's last row), kept in a
         // register so the walk reads row_ptr once per row, not per nonzero
         int next_end = ly < ly_end ? row_end(s_rp, rpo, ly, x0) : INT_MAX;
+        // fused dval: this lane's VW values of dv_x's current row
+        const X* __restrict__ dvx = static_cast<const X*>(a.dv_x);
+        X* __restrict__ dvo = static_cast<X*>(a.dv_out);
+        X xrow[VW];
+        int xrow_of = -1;
+        const int* s_perm = reinterpret_cast<const int*>(ws + perm_offset);
+        const unsigned gmask = LPG == 32 ? 0xFFFFFFFFu : (((1u << LPG) - 1u) << (g * LPG));
         auto consume = [&](int c, const X (&xr)[CH][VW], const V (&vv)[CH]) {
 #pragma unroll
             for (int t = 0; t < CH; ++t) {
@@ -240,6 +255,21 @@ struct SpmmTile {
                     const P av = to_p(vv[t]);
 #pragma unroll
                     for (int v = 0; v < VW; ++v) acc[v].add(av * (P)xr[t][v]);
+                    if (DV) {
+                        if (y0 + ly != xrow_of) {  // uniform within the group
+                            xrow_of = y0 + ly;
+                            ld_vec<VW>(dvx + (size_t)xrow_of * a.dv_ldx + j0, xrow);
+                        }
+                        // in the x type: VW fused multiply-adds per lane, then a
+                        // tree over the group's lanes (error within
+                        // (VW + log2 LPG) roundings of sum |g x|)
+                        X dd = (X)0;
+#pragma unroll
+                        for (int v = 0; v < VW; ++v) dd = fma(xr[t][v], xrow[v], dd);
+#pragma unroll
+                        for (int o = LPG / 2; o > 0; o >>= 1) dd += __shfl_xor_sync(gmask, dd, o);
+                        if (jl == 0) dvo[s_perm[col_o + e]] = dd;
+                    }
                 }
             }
         };
@@ -399,9 +429,9 @@ struct SpmmTile {
     }
 };
 
-template <int DT, int K, int VW, int ITEMS, int WARPS>
+template <int DT, int K, int VW, int ITEMS, int WARPS, bool DV>
 __global__ void __launch_bounds__(WARPS * 32) spmm_kernel(const SpmmLaunch a) {
-    using T = SpmmTile<DT, K, VW, ITEMS>;
+    using T = SpmmTile<DT, K, VW, ITEMS, DV>;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned s_epoch;
     const int lane = threadIdx.x & 31;
@@ -430,7 +460,7 @@ __global__ void __launch_bounds__(WARPS * 32) spmm_kernel(const SpmmLaunch a) {
         }
         const SpmmDesc& d = *dp;
         const int lt = u - d.tile_begin;
-        T::issue(d, lt, ws, bar, lane);
+        T::issue(d, lt, ws, bar, lane, a.dv_perm);
         const bool ok = __all_sync(0xFFFFFFFFu, mbar_wait_bounded(bar, phase, a.state));
         phase ^= 1u;
         __syncwarp();
@@ -442,15 +472,15 @@ __global__ void __launch_bounds__(WARPS * 32) spmm_kernel(const SpmmLaunch a) {
 
 namespace {
 
-template <int DT, int K, int VW, int ITEMS, int WARPS>
+template <int DT, int K, int VW, int ITEMS, int WARPS, bool DV>
 int launch_spmm_cfg(const SpmmLaunch& a, cudaStream_t s) {
-    using T = SpmmTile<DT, K, VW, ITEMS>;
+    using T = SpmmTile<DT, K, VW, ITEMS, DV>;
     constexpr size_t smem = T::bytes * WARPS;
     static int grid_cap[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmm: device ordinal >= 64");
-    auto kern = spmm_kernel<DT, K, VW, ITEMS, WARPS>;
+    auto kern = spmm_kernel<DT, K, VW, ITEMS, WARPS, DV>;
     if (grid_cap[dev] == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -481,8 +511,12 @@ int launch_spmm_cfg(const SpmmLaunch& a, cudaStream_t s) {
 // Configurations: (K, VW, ITEMS).  WARPS = 4.
 template <int DT>
 int launch_spmm_dt(int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s) {
-#define MERBIT_SPMM_CASE(KK, VV, II) \
-    if (k == KK && vw == VV && items == II) return launch_spmm_cfg<DT, KK, VV, II, 4>(a, s);
+    constexpr bool kDv = DT != MERBIT_BF16;  // fused dval: F64 and F32 plans
+    if (a.dv_out && !kDv) return fail(MERBIT_ERR_UNSUPPORTED, "spmm: fused dval needs F64 or F32 values");
+#define MERBIT_SPMM_CASE(KK, VV, II)                                                  \
+    if (k == KK && vw == VV && items == II)                                           \
+        return a.dv_out ? launch_spmm_cfg<DT, KK, VV, II, 4, kDv>(a, s)                \
+                        : launch_spmm_cfg<DT, KK, VV, II, 4, false>(a, s);
     MERBIT_SPMM_CASE(1, 1, 256)
     MERBIT_SPMM_CASE(2, 1, 256)
     MERBIT_SPMM_CASE(2, 2, 256)

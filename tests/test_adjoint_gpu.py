@@ -150,3 +150,59 @@ def test_dval_strided_operands(dtype, k, ld):
     den = O.dval(A.row_ptr, A.col, np.abs(Gh).astype(np.float64), np.abs(Xh).astype(np.float64))
     tol = 1e-13 if dtype == "f64" else 1e-6
     assert (np.abs(out.cpu().numpy() - ref) / np.maximum(den, 1e-300)).max() <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("k", [1, 2, 4, 8, 16, 32])
+def test_fused_backward_matches_oracle(dtype, k):
+    """merbit_spmm_dval: dX = A^T G and dval from one launch, against the
+    oracle, on the power-law instance (long rows span many tiles)."""
+    A = synth.workload("zipf_small")
+    nt = np.float64 if dtype == "f64" else np.float32
+    X = synth.uniform(4, A.ncol * k).reshape(A.ncol, k).astype(nt)
+    G = synth.normal(6, A.nrow * k).reshape(A.nrow, k).astype(nt)
+    rp, col, v = to_cuda(A, dtype)
+    M = SparseMatrix(rp, col, v)
+    out = M.backward_fused(torch.from_numpy(G).cuda(), torch.from_numpy(X).cuda())
+    assert out is not None
+    dX, dv = (t.cpu().numpy() for t in out)
+    tol = 1e-13 if dtype == "f64" else 1e-6
+    vals = stored_values(A, dtype)
+    ref = O.spmm_t(A.row_ptr, A.col, vals, G, A.ncol)
+    den = O.spmm_t(A.row_ptr, A.col, np.abs(vals.astype(np.float64)), np.abs(G.astype(np.float64)),
+                   A.ncol)
+    assert (np.abs(dX - ref) / np.maximum(den, 1e-300)).max() <= tol
+    refv = O.dval(A.row_ptr, A.col, G, X)
+    denv = O.dval(A.row_ptr, A.col, np.abs(G.astype(np.float64)), np.abs(X.astype(np.float64)))
+    assert (np.abs(dv - refv) / np.maximum(denv, 1e-300)).max() <= tol
+
+
+@pytest.mark.gpu
+def test_fused_backward_strided_x_and_fallbacks():
+    A = _diff_instance()
+    rp, col, v = to_cuda(A, "f32")
+    M = SparseMatrix(rp, col, v)
+    k = 16
+    Xw = torch.from_numpy(synth.uniform(2, A.ncol * 18).reshape(A.ncol, 18).astype(np.float32)).cuda()
+    X = Xw[:, 1:17]  # leading dimension 18, offset by one float: narrower vector loads
+    G = torch.from_numpy(synth.normal(3, A.nrow * k).reshape(A.nrow, k).astype(np.float32)).cuda()
+    from merbit_b200 import _check, _dptr, _stream_ptr, lib
+
+    T = M.transpose_plan()
+    dX = torch.empty(A.ncol, k, device="cuda")
+    dv = torch.empty(A.nnz, device="cuda")
+    _check(lib().merbit_spmm_dval(T._h, k, _dptr(G), k, _dptr(X), 18, _dptr(dX), k, _dptr(dv),
+                                  _stream_ptr(None)))
+    ref_dx = T.spmm(G)
+    ref_dv = M.dval(G, X.contiguous())
+    assert torch.allclose(dX, ref_dx, rtol=1e-5, atol=1e-6)
+    assert torch.allclose(dv, ref_dv, rtol=1e-5, atol=1e-6)
+    # k outside {1,2,4,...,32} and bf16 values are declined
+    assert M.backward_fused(G[:, :3].contiguous(), X[:, :3].contiguous()) is None
+    rpb, colb, vb = to_cuda(A, "bf16")
+    Mb = SparseMatrix(rpb, colb, vb)
+    assert Mb.backward_fused(G, X.contiguous()) is None
+    # the plan of A itself is not a transpose plan
+    assert lib().merbit_spmm_dval(M.plan._h, k, _dptr(G), k, _dptr(X), 18, _dptr(dX), k, _dptr(dv),
+                                  _stream_ptr(None)) == 1
