@@ -48,7 +48,7 @@ if ROOT not in sys.path:
 
 METRIC = "SpMV GB/s (% of HBM peak) & GFLOP/s; mixed/batched vs plain FP64 at 1e-6 rel"
 FALLBACK_HBM_GBS = 6650.0
-KERNEL_OF_KIND = {0: "spmv_tile_kernel", 1: "spmv_warp_kernel"}
+KERNEL_OF_KIND = {0: "spmv_tile_kernel", 1: "spmv_warp_kernel", 3: "spmv_rows_kernel"}
 
 
 def parse_args():
@@ -294,7 +294,10 @@ def run_ours(args):
     vals = torch.from_numpy(A.vals).to(dev).to(vt)
     xd = torch.from_numpy(x).to(dev).to(xt)
     yd = torch.empty(A.nrow, dtype=xt, device=dev)
-    plan = mb.Plan(rp, col, vals, ncol=A.ncol)
+    torch.cuda.synchronize(dev)
+    t_plan0 = time.perf_counter()
+    plan = mb.Plan(rp, col, vals, ncol=A.ncol)  # validates, partitions; synchronizes
+    t_plan = time.perf_counter() - t_plan0
     if args.config >= 0:
         plan.set_config(args.config)
     elif not args.no_tune:
@@ -407,6 +410,7 @@ def run_ours(args):
         "value_l2_flushed": round(ws * B / (ms_cold * 1e-3) / 1e9, 2),
         "algorithmic_bytes_per_step": B,
         "plan_metadata_bytes": info.metadata_bytes,
+        "plan_build_ms_host_wall": round(t_plan * 1e3, 3),
         "gpu_launches": args.steps,
         "roofline": {
             "bound": "hbm",
@@ -785,7 +789,56 @@ def run_reference(args):
                 "ms_per_spmv": round(float(ms), 5), "reps": 400,
                 "plan_build_s_host_wall": round(t_plan, 4),
             }
+        out["competitors_gpu"] = competitors(A, rp, col, v, xd, yd, zd, B, dev)
     print(json.dumps(out), flush=True)
+
+
+def competitors(A, rp, col, v, xd, yd, zd, B, dev):
+    """Run-only comparisons on the same matrix (GB/s of the same algorithmic
+    bytes): the reference Merbit kernel with 64-bit lane descriptors
+    (SIGMA 20), and cuSPARSE through torch.sparse (CSR SpMV)."""
+    import ctypes as C
+
+    import torch
+
+    from oracle import oracle as O
+
+    res = {}
+    R = O.ref()
+    s = torch.cuda.current_stream(dev)
+    if R is not None:
+        t, ln = C.c_int(), C.c_int()
+        R.ref_tile_dims(A.nrow, A.nnz, 20, C.byref(t), C.byref(ln))
+        tx = torch.zeros(t.value + 1, dtype=torch.int32, device=dev)
+        ty = torch.zeros(t.value + 1, dtype=torch.int32, device=dev)
+        desc = torch.zeros(max(ln.value, 1), dtype=torch.int64, device=dev)
+        if R.ref_tile_build(20, rp.data_ptr(), A.nrow, A.nnz, tx.data_ptr(), ty.data_ptr(),
+                            desc.data_ptr()) == 0:
+            args = (0, col.data_ptr(), v.data_ptr(), A.nrow, A.nnz, tx.data_ptr(), ty.data_ptr(),
+                    desc.data_ptr(), xd.data_ptr(), yd.data_ptr(), zd.data_ptr())
+            R.ref_merbit_time_sigma(20, *args, 10, s.cuda_stream)
+            ms = R.ref_merbit_time_sigma(20, *args, 200, s.cuda_stream)
+            res["merbit_kernel_sigma20"] = {"value": round(B / (ms * 1e-3) / 1e9, 2),
+                                            "unit": "GB/s", "ms_per_spmv": round(float(ms), 5)}
+        del tx, ty, desc
+    try:
+        Acsr = torch.sparse_csr_tensor(rp, col, v, size=(A.nrow, A.ncol))
+        for _ in range(3):
+            torch.mv(Acsr, xd)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(50):
+            torch.mv(Acsr, xd)
+        e1.record(s)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / 50
+        res["cusparse_csr_spmv"] = {"value": round(B / (ms * 1e-3) / 1e9, 2), "unit": "GB/s",
+                                    "ms_per_spmv": round(ms, 5),
+                                    "via": "torch.mv on a torch.sparse_csr_tensor (cuSPARSE SpMV)"}
+    except RuntimeError as e:  # a torch build without sparse CSR on CUDA
+        res["cusparse_csr_spmv"] = {"unavailable": str(e).splitlines()[0][:120]}
+    return res
 
 
 def main():

@@ -70,7 +70,7 @@ typedef struct merbit_plan_info {
     int32_t tile_items;      /* merge items (row ends + nonzeros) per tile */
     int32_t num_tiles;
     int32_t vectorized;      /* 1 when 128-bit loads of col_idx/vals are used */
-    int32_t kind;            /* 0: CTA-tile kernel, 1: warp-tile kernel */
+    int32_t kind;            /* 0: CTA-tile kernel, 1: warp-tile kernel, 3: row-group kernel */
     int32_t l1_carveout;     /* warp-tile kernel: preferred shared-memory carveout, percent
                                 (0: driver default, all shared memory) */
     int32_t gather_l2_only;  /* 1: x gathers bypass L1 allocation (ld.global.cg) */
@@ -124,6 +124,8 @@ int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream)
  * 32*items_per_thread items (needs 16-byte aligned row_ptr/col_idx/vals);
  * warp-tile entries also differ in the shared-memory / L1 split they launch
  * with and in the cache hint of the x gathers (merbit_plan_get_info).
+ * kind 3 = row groups: items_per_thread lanes own one row (no merge-path
+ * tiles; tile_items 0), for short, even rows such as stencils.
  * merbit_plan_set_config forces one (MERBIT_ERR_INVALID if the plan's
  * arrays do not allow it); it builds that tile size's partition on first
  * use, synchronizing `stream`. */

@@ -368,7 +368,8 @@ class Plan:
 
     def configs(self) -> list[tuple[int, int, int, int]]:
         """[(index, kind, block, items_per_thread)] of the kernel configurations
-        this plan can run (kind 1 needs 16-byte aligned arrays)."""
+        this plan can run (kind 0 CTA tiles, 1 warp tiles -- needs 16-byte
+        aligned arrays --, 3 row groups with items_per_thread lanes per row)."""
         out = []
         for i in range(lib().merbit_num_configs(self.dtype)):
             k, b, p, ok = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()

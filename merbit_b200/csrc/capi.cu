@@ -73,6 +73,10 @@ int plan_config_ok(merbit_plan_s* p, int idx, bool* ok, cudaStream_t s) {
     *ok = false;
     const SpmvConfig c = spmv_config(p->dtype, idx);
     if (!spmv_config_allowed(c, p->vec)) return MERBIT_OK;
+    if (c.kind == 3) {  // row groups: no partition, any matrix
+        *ok = true;
+        return MERBIT_OK;
+    }
     const Partition* part = nullptr;
     int st = plan_partition(p, spmv_tile_items(c), &part, s);
     if (st != MERBIT_OK) return st;
@@ -117,10 +121,13 @@ int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta
              cudaStream_t s, const void* z = nullptr, double* residual = nullptr) {
     const SpmvConfig c = spmv_config(p->dtype, cfg);
     const Partition* part = nullptr;
-    int st = plan_partition(p, spmv_tile_items(c), &part, s);
-    if (st != MERBIT_OK) return st;
+    int st = MERBIT_OK;
+    if (c.kind != 3) {
+        st = plan_partition(p, spmv_tile_items(c), &part, s);
+        if (st != MERBIT_OK) return st;
+    }
     if (residual) {
-        st = plan_partials(p, part->num_tiles);
+        st = plan_partials(p, part ? part->num_tiles : 0);
         if (st != MERBIT_OK) return st;
     }
     SpmvLaunch a;
@@ -129,14 +136,14 @@ int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta
     a.vals = p->vals;
     a.x = x;
     a.y = y;
-    a.coords = part->coords;
+    a.coords = part ? part->coords : nullptr;
     a.slots = p->carry;
     a.xch = p->carry + 2 * (size_t)p->slots;
     a.nslots = p->slots;
     a.state = p->state;
     a.nrow = p->nrow;
     a.nnz = p->nnz;
-    a.num_tiles = part->num_tiles;
+    a.num_tiles = part ? part->num_tiles : 0;
     a.alpha = alpha;
     a.beta = beta;
     a.z = z;

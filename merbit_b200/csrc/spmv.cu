@@ -251,7 +251,8 @@ __global__ void __launch_bounds__(BLOCK) spmv_tile_kernel(const SpmvLaunch a) {
 // ---------------------------------------------------------------------------
 // Configuration table.  kind 0 = this CTA-tile kernel (tile = block*ipt
 // items), kind 1 = the warp-tile kernel of spmv_warp.cu (tile = 32*ipt items,
-// block/32 warps per CTA, needs 16-byte aligned col_idx/vals).
+// block/32 warps per CTA, needs 16-byte aligned col_idx/vals), kind 3 = the
+// row-group kernel of spmv_rows.cu (ipt = lanes per row, no tiles).
 // ---------------------------------------------------------------------------
 namespace {
 // Items per thread are odd: a lane's segment then starts an odd number of
@@ -269,7 +270,11 @@ constexpr SpmvConfig kCfgF64[] = {
     {1, 128, 15, 1, 0, 0},           {1, 256, 11, 1, 0, 0},
     {1, 256, 7, 1, 0, 0},            {1, 128, 23, 1, 0, 0},
     {0, 256, 7, 1, 0, 0},            {0, 256, 11, 1, 0, 0},
-    {0, 128, 9, 1, 0, 0}};
+    {0, 128, 9, 1, 0, 0},
+    {3, 256, 4, 1, 0, 0},            {3, 256, 8, 1, 0, 0},
+    {3, 256, 16, 1, 0, 0},           {3, 256, 32, 1, 0, 0},
+    {3, 256, 8, 1, 0, 1},            {3, 256, 16, 1, 0, 1},
+    {3, 256, 2, 1, 0, 0}};
 constexpr SpmvConfig kCfgF32[] = {
     {1, 256, 15, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1, 1},
     {1, 256, 11, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1Max, 1},
@@ -277,7 +282,11 @@ constexpr SpmvConfig kCfgF32[] = {
     {1, 128, 15, 1, 0, 0},           {1, 256, 11, 1, 0, 0},
     {1, 256, 7, 1, 0, 0},            {1, 128, 23, 1, 0, 0},
     {0, 256, 11, 1, 0, 0},           {0, 256, 7, 1, 0, 0},
-    {0, 256, 15, 1, 0, 0}};
+    {0, 256, 15, 1, 0, 0},
+    {3, 256, 4, 1, 0, 0},            {3, 256, 8, 1, 0, 0},
+    {3, 256, 16, 1, 0, 0},           {3, 256, 32, 1, 0, 0},
+    {3, 256, 8, 1, 0, 1},            {3, 256, 16, 1, 0, 1},
+    {3, 256, 2, 1, 0, 0}};
 
 template <int DT, int BLOCK, int IPT, bool VEC, bool RES>
 int launch_one_k(const SpmvLaunch& a, cudaStream_t s) {
@@ -331,20 +340,25 @@ SpmvConfig spmv_config(int dtype, int idx) {
     return dtype == MERBIT_F64 ? kCfgF64[idx] : kCfgF32[idx];
 }
 
-int spmv_tile_items(const SpmvConfig& c) { return c.kind != 0 ? 32 * c.ipt : c.block * c.ipt; }
+// kind 3 has no merge-path tiles (0: no partition to build)
+int spmv_tile_items(const SpmvConfig& c) {
+    return c.kind == 3 ? 0 : c.kind == 1 ? 32 * c.ipt : c.block * c.ipt;
+}
 
-bool spmv_config_allowed(const SpmvConfig& c, bool vec) { return vec || c.kind == 0; }
+bool spmv_config_allowed(const SpmvConfig& c, bool vec) { return vec || c.kind == 0 || c.kind == 3; }
 
 int spmv_config_row_cap(const SpmvConfig& c) {
-    return c.kind != 0 ? warp_rp_cap(c.ipt) - 8 : INT_MAX;
+    return c.kind == 1 ? warp_rp_cap(c.ipt) - 8 : INT_MAX;
 }
 
 
 int spmv_warp_launch(int dtype, const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s);
+int spmv_rows_launch(int dtype, const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s);
 
 int spmv_launch(int dtype, int cfg, bool vec, const SpmvLaunch& a, cudaStream_t s) {
-    if (a.num_tiles <= 0) return MERBIT_OK;
     const SpmvConfig c = spmv_config(dtype, cfg);
+    if (c.kind == 3) return spmv_rows_launch(dtype, c, a, s);  // no tiles
+    if (a.num_tiles <= 0) return MERBIT_OK;
     if (!spmv_config_allowed(c, vec)) return fail(MERBIT_ERR_INVALID, "spmv: config needs aligned arrays");
     if (c.kind != 0) return spmv_warp_launch(dtype, c, a, s);
     switch (dtype) {

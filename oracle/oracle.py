@@ -79,6 +79,9 @@ def ref():
             R.ref_merbit_time.argtypes = [C.c_int, _p, _p, C.c_int, C.c_int, _p, _p, _p, _p, _p,
                                           _p, C.c_int, _p]
             R.ref_merbit_time.restype = C.c_float
+            R.ref_merbit_time_sigma.argtypes = [C.c_int, C.c_int, _p, _p, C.c_int, C.c_int, _p,
+                                                _p, _p, _p, _p, _p, C.c_int, _p]
+            R.ref_merbit_time_sigma.restype = C.c_float
             _ref = R
     return _ref
 

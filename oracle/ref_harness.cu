@@ -11,9 +11,10 @@
  *   ref_merbit_spmv    one merbit_kernel<V,256,14>      include/tile.cuh:476-561,596-601
  *                      launch after zeroing y and z, as Fun_Merbit does
  *                      before its loop (include/tile.cuh:597)
+ *   ref_merbit_time[_sigma]  mean time of repeated launches (SIGMA 14, 20)
  *
  * Used by tests/ (GPU parity against the reference kernel), the golden
- * fixture script and nothing else.
+ * fixture script and bench.py's reference arm, and nothing else.
  */
 #include "tile.cuh"
 
@@ -85,16 +86,16 @@ int ref_merbit_spmv(int dtype, const int* d_colidx, const void* d_vals, int nrow
     return e == cudaSuccess ? 0 : (int)e;
 }
 
-/* Same kernel, launched `reps` times back to back on `stream` with the y/z
- * ping-pong of Fun_Merbit (include/tile.cuh:599-603); returns the mean
- * milliseconds per launch measured with CUDA events on that stream. */
-float ref_merbit_time(int dtype, const int* d_colidx, const void* d_vals, int nrow, int nnz,
-                      const unsigned* d_tile_x, const unsigned* d_tile_y, const void* d_lane_desc,
-                      const void* d_x, void* d_y, void* d_z, int reps, void* stream) {
+}  // extern "C"
+
+template <unsigned SIGMA>
+static float time_sigma(int dtype, const int* d_colidx, const void* d_vals, int nrow, int nnz,
+                        const unsigned* d_tile_x, const unsigned* d_tile_y,
+                        const void* d_lane_desc, const void* d_x, void* d_y, void* d_z, int reps,
+                        cudaStream_t s) {
     int tile_num, lane_num;
-    ref_tile_dims(nrow, nnz, 14, &tile_num, &lane_num);
+    ref_tile_dims(nrow, nnz, (int)SIGMA, &tile_num, &lane_num);
     const int grid = (lane_num + 256 - 1) / 256;
-    cudaStream_t s = (cudaStream_t)stream;
     size_t vs = dtype == 0 ? sizeof(double) : sizeof(float);
     cudaMemsetAsync(d_y, 0, vs * (size_t)nrow, s);
     cudaMemsetAsync(d_z, 0, vs * (size_t)nrow, s);
@@ -104,14 +105,14 @@ float ref_merbit_time(int dtype, const int* d_colidx, const void* d_vals, int nr
     cudaEventRecord(a, s);
     for (int r = 0; r < reps; ++r) {
         if (dtype == 0)
-            merbit_kernel<double, 256, 14><<<grid, 256, 0, s>>>(
+            merbit_kernel<double, 256, SIGMA><<<grid, 256, 0, s>>>(
                 d_colidx, (const double*)d_vals, nrow, nnz, d_tile_x, d_tile_y,
-                (const DescTypeT<14>*)d_lane_desc, tile_num, lane_num, 1.0, (const double*)d_x,
+                (const DescTypeT<SIGMA>*)d_lane_desc, tile_num, lane_num, 1.0, (const double*)d_x,
                 (double*)d_y, (double*)d_z);
         else
-            merbit_kernel<float, 256, 14><<<grid, 256, 0, s>>>(
+            merbit_kernel<float, 256, SIGMA><<<grid, 256, 0, s>>>(
                 d_colidx, (const float*)d_vals, nrow, nnz, d_tile_x, d_tile_y,
-                (const DescTypeT<14>*)d_lane_desc, tile_num, lane_num, 1.0f, (const float*)d_x,
+                (const DescTypeT<SIGMA>*)d_lane_desc, tile_num, lane_num, 1.0f, (const float*)d_x,
                 (float*)d_y, (float*)d_z);
         void* t = d_y;
         d_y = d_z;
@@ -124,6 +125,33 @@ float ref_merbit_time(int dtype, const int* d_colidx, const void* d_vals, int nr
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return reps > 0 ? ms / reps : 0.f;
+}
+
+extern "C" {
+
+/* Same kernel, launched `reps` times back to back on `stream` with the y/z
+ * ping-pong of Fun_Merbit (include/tile.cuh:599-603); returns the mean
+ * milliseconds per launch measured with CUDA events on that stream. */
+float ref_merbit_time(int dtype, const int* d_colidx, const void* d_vals, int nrow, int nnz,
+                      const unsigned* d_tile_x, const unsigned* d_tile_y, const void* d_lane_desc,
+                      const void* d_x, void* d_y, void* d_z, int reps, void* stream) {
+    return time_sigma<14>(dtype, d_colidx, d_vals, nrow, nnz, d_tile_x, d_tile_y, d_lane_desc,
+                          d_x, d_y, d_z, reps, (cudaStream_t)stream);
+}
+
+/* As ref_merbit_time for SIGMA 14 or 20 (20: 64-bit lane descriptors,
+ * include/tile.cuh:6-25); -1 for another SIGMA. */
+float ref_merbit_time_sigma(int sigma, int dtype, const int* d_colidx, const void* d_vals,
+                            int nrow, int nnz, const unsigned* d_tile_x, const unsigned* d_tile_y,
+                            const void* d_lane_desc, const void* d_x, void* d_y, void* d_z,
+                            int reps, void* stream) {
+    if (sigma == 14)
+        return time_sigma<14>(dtype, d_colidx, d_vals, nrow, nnz, d_tile_x, d_tile_y, d_lane_desc,
+                              d_x, d_y, d_z, reps, (cudaStream_t)stream);
+    if (sigma == 20)
+        return time_sigma<20>(dtype, d_colidx, d_vals, nrow, nnz, d_tile_x, d_tile_y, d_lane_desc,
+                              d_x, d_y, d_z, reps, (cudaStream_t)stream);
+    return -1.f;
 }
 
 }  // extern "C"

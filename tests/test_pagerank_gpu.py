@@ -50,7 +50,7 @@ def test_pagerank_step_every_config(dtype, workload):
     rp, col, v = to_cuda(A, dtype)
     plan = mb.Plan(rp, col, v)
     cfgs = plan.configs()
-    assert {0, 1} <= {k for _, k, _, _ in cfgs}
+    assert {0, 1, 3} <= {k for _, k, _, _ in cfgs}
     for idx, _, _, _ in cfgs:
         plan.set_config(idx)
         _check_step(A, dtype, plan, x, t)

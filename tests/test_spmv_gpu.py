@@ -65,10 +65,10 @@ def test_spmv_every_config(dtype, workload):
     plan = mb.Plan(rp, col, v)
     xd = torch.from_numpy(x).cuda()
     cfgs = plan.configs()
-    assert {0, 1} <= {k for _, k, _, _ in cfgs}
+    assert {0, 1, 3} <= {k for _, k, _, _ in cfgs}
     for idx, kind, block, ipt in cfgs:
         plan.set_config(idx)
-        assert plan.info().tile_items == (32 * ipt if kind != 0 else block * ipt)
+        assert plan.info().tile_items == {0: block * ipt, 1: 32 * ipt, 3: 0}[kind]
         y = plan.spmv(xd)
         torch.cuda.synchronize()
         plan.check()
