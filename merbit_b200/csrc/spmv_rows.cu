@@ -4,7 +4,7 @@
 // path walk costs more than it saves: every item goes through shared memory
 // twice and every row end through a scan.  Here a group of LPR lanes owns a
 // whole row: the lanes read the row's col_idx/vals coalesced (lane j takes
-// nonzeros j, j+LPR, ...), keep UNR gathers of x in flight, accumulate with
+// nonzeros j, j+LPR, ...), keep up to 8 gathers of x in flight, accumulate with
 // the dtype's policy (F64: double; F32/BF16: TwoSum), and the group combines
 // its lane sums by a fixed butterfly in double.  No row spans two groups, so
 // there are no carries, no atomics and no shared memory; results are
@@ -68,7 +68,9 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch 
     using P = typename Pr::P;
     using Acc = typename Pr::Acc;
     constexpr int RPW = 32 / LPR;  // rows per warp step
-    constexpr int UNR = 4;         // gathers in flight per lane
+    // loads in flight per lane and step: a 27-point row at 4 lanes per row
+    // is one step
+    constexpr int UNR = LPR <= 4 ? 8 : 4;
     const int lane = threadIdx.x & 31;
     const int grp = lane / LPR, jl = lane % LPR;
     const unsigned gmask = LPR == 32 ? 0xFFFFFFFFu : (((1u << LPR) - 1u) << (grp * LPR));
@@ -85,22 +87,25 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch 
         acc.zero();
         if (r < a.nrow) {
             const int s = __ldg(rp + r), e = __ldg(rp + r + 1);
-            int i = s + jl;
-            for (; i + (UNR - 1) * LPR < e; i += UNR * LPR) {
+            // steps of UNR * LPR nonzeros, predicated at the row end, so all
+            // of a step's loads are in flight together
+            for (int i = s + jl; i < e; i += UNR * LPR) {
                 int c[UNR];
                 V v[UNR];
 #pragma unroll
                 for (int u = 0; u < UNR; ++u) {
-                    c[u] = __ldcs(col + i + u * LPR);
-                    v[u] = __ldcs(vals + i + u * LPR);
+                    const int k = i + u * LPR;
+                    c[u] = k < e ? __ldcs(col + k) : -1;
+                    v[u] = k < e ? __ldcs(vals + k) : V(0);
                 }
                 X xg[UNR];
 #pragma unroll
-                for (int u = 0; u < UNR; ++u) xg[u] = CG ? __ldcg(xv + c[u]) : __ldg(xv + c[u]);
+                for (int u = 0; u < UNR; ++u)
+                    xg[u] = c[u] >= 0 ? (CG ? __ldcg(xv + c[u]) : __ldg(xv + c[u])) : (X)0;
 #pragma unroll
-                for (int u = 0; u < UNR; ++u) acc.add(to_p(v[u]) * (P)xg[u]);
+                for (int u = 0; u < UNR; ++u)
+                    if (c[u] >= 0) acc.add(to_p(v[u]) * (P)xg[u]);
             }
-            for (; i < e; i += LPR) acc.add(to_p(__ldcs(vals + i)) * (P)__ldg(xv + __ldcs(col + i)));
         }
         double t = acc.value();
 #pragma unroll
