@@ -15,12 +15,18 @@
  *                         Fun_Merbit (sort is the caller's; see merbit_coo_to_csr)
  *   merbit_spmv           merbit_kernel launch            include/tile.cuh:476-561,596-603
  *                         (y = alpha*A*x; beta extends it)
- *   merbit_spmm           (k right-hand sides; no reference counterpart, same kernel family)
- *   merbit_spmm_t         adjoint dX = A^T G              (no reference counterpart)
- *   merbit_dval           adjoint dval = G[row].X[col]    (no reference counterpart)
- *   merbit_coo_to_csr     GRAPH::sort(false) +            src/class.cu:143-177,
- *                         cusparseXcoo2csr                 include/tile.cuh:571-574
- *   merbit_pagerank_step  PARAMETER damping scaffold      include/class.cuh:119-146
+ *   merbit_coo_sort       GRAPH::sort                     src/class.cu:143-177
+ *   merbit_coo_to_csr     cusparseXcoo2csr in Fun_Merbit  include/tile.cuh:571-574
+ *   merbit_outdegree_values  Fun_Values (loader weights)  src/class.cu:2-34
+ *   merbit_pagerank_step  PARAMETER damping scaffold      include/class.cuh:119-157
+ *
+ * With no reference counterpart (same kernel family):
+ *   merbit_spmm, merbit_batch_*   k right-hand sides; many matrices per launch
+ *   merbit_plan_transpose + merbit_spmm, merbit_dval, merbit_spmm_dval
+ *                         adjoints dX = A^T G and dval = G[row].X[col]
+ *   merbit_plan_tune, merbit_plan_set_config   the configuration table
+ *   merbit_spmv_noalloc   one SpMV that allocates nothing
+ *   merbit_plan_check, merbit_plan_selftest_wait   device-side failure status
  *
  * Threading: a plan may be used from any host thread, but launches that use
  * the same plan must be ordered on the device (one stream, or ordered by

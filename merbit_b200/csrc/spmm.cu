@@ -9,7 +9,7 @@
 // lane: 1, 2 or 4); each group walks its own segment of ITEMS/G merge items
 // (G groups per warp), lane j of a group owning RHS columns
 // [j*VW, j*VW + VW).  The x rows of the next CH nonzeros are gathered while
-// the current CH are accumulated, so gathers overlap the walk.  A rows that
+// the current CH are accumulated, so gathers overlap the walk.  A row that
 // ends inside a segment is written directly (coalesced across the group's
 // lanes); the group segmented scan (shuffles with stride K/VW) finishes the
 // rows split between groups, and rows split between tiles are finished
@@ -23,6 +23,11 @@
 // persistent cooperative grid take tiles round-robin, so one launch covers
 // the whole batch, and the launch can be captured in a CUDA graph and
 // replayed (carry slots are per launch parity, as in the SpMV).
+//
+// Fused backward (DV, merbit_spmm_dval): run on the transpose plan of A, the
+// walk also forms dL/dval for each nonzero from the G row it has just
+// gathered and the current row of X, and stores it through the transpose
+// permutation (staged by TMA with the tile's col and vals).
 #include <type_traits>
 
 #include "merbit_internal.cuh"

@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch 
     constexpr int RPW = 32 / LPR;  // rows per warp step
     // loads in flight per lane and step: a 27-point row at 4 lanes per row
     // is one step
-    constexpr int UNR = LPR <= 4 ? 8 : 4;
+    constexpr int UNR = LPR <= 2 ? 16 : (LPR <= 4 ? 8 : 4);
     const int lane = threadIdx.x & 31;
     const int grp = lane / LPR, jl = lane % LPR;
     const unsigned gmask = LPR == 32 ? 0xFFFFFFFFu : (((1u << LPR) - 1u) << (grp * LPR));
