@@ -83,6 +83,84 @@ __device__ __forceinline__ unsigned long long dbits(double v) {
 
 }  // namespace
 
+// The VW accumulators of one lane.  Generic: one Acc per column.
+template <class Acc, int VW, typename P, typename X>
+struct AccRow {
+    Acc a[VW];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int v = 0; v < VW; ++v) a[v].zero();
+    }
+    __device__ __forceinline__ void add(P av, const X (&x)[VW]) {
+#pragma unroll
+        for (int v = 0; v < VW; ++v) a[v].add(av * (P)x[v]);
+    }
+    __device__ __forceinline__ double value(int v) const { return a[v].value(); }
+};
+
+// TwoSum accumulators of an even number of columns, two columns per packed
+// f32x2 instruction (sm_100).  Every operation rounds as the scalar TwoSum of
+// AccTwoSum does (products rounded, then s + p with its exact error added
+// to c), so the results are bit-identical to the scalar form with half the
+// instructions.
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+template <int VW>
+struct AccRow<AccTwoSum, VW, float, float> {
+    static_assert(VW % 2 == 0, "packed TwoSum needs an even width");
+    unsigned long long s[VW / 2], c[VW / 2];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int h = 0; h < VW / 2; ++h) s[h] = c[h] = 0ull;  // +0.0f, +0.0f
+    }
+    __device__ __forceinline__ void add(float av, const float (&x)[VW]) {
+        const unsigned long long a2 = f2_pack(av, av);
+#pragma unroll
+        for (int h = 0; h < VW / 2; ++h) {
+            const unsigned long long p = f2_mul(a2, f2_pack(x[2 * h], x[2 * h + 1]));
+            const unsigned long long t = f2_add(s[h], p);
+            const unsigned long long bp = f2_sub(t, s[h]);
+            const unsigned long long e = f2_add(f2_sub(s[h], f2_sub(t, bp)), f2_sub(p, bp));
+            s[h] = t;
+            c[h] = f2_add(c[h], e);
+        }
+    }
+    __device__ __forceinline__ double value(int v) const {
+        float s0, s1, c0, c1;
+        f2_unpack(s[v / 2], s0, s1);
+        f2_unpack(c[v / 2], c0, c1);
+        return (v & 1) ? (double)s1 + (double)c1 : (double)s0 + (double)c0;
+    }
+};
+template <>
+struct AccRow<AccTwoSum, 1, float, float> {
+    AccTwoSum a;
+    __device__ __forceinline__ void zero() { a.zero(); }
+    __device__ __forceinline__ void add(float av, const float (&x)[1]) { a.add(av * x[0]); }
+    __device__ __forceinline__ double value(int) const { return a.value(); }
+};
+
 // DV: also form dL/dval for each nonzero (SpmmLaunch::dv_*), from the x row
 // the walk gathers anyway and the current row of dv_x.
 template <int DT, int K, int VW, int ITEMS, bool DV = false>
@@ -201,9 +279,8 @@ struct SpmmTile {
         search(ds, lx, ly);
         search(de, lx_end, ly_end);
 
-        Acc acc[VW];
-#pragma unroll
-        for (int v = 0; v < VW; ++v) acc[v].zero();
+        AccRow<Acc, VW, P, X> acc;
+        acc.zero();
         int first_row = -1;
         double first_val[VW];
 #pragma unroll
@@ -212,14 +289,13 @@ struct SpmmTile {
             if (first_row < 0) {
                 first_row = r;
 #pragma unroll
-                for (int v = 0; v < VW; ++v) first_val[v] = acc[v].value();
+                for (int v = 0; v < VW; ++v) first_val[v] = acc.value(v);
             } else {
 #pragma unroll
                 for (int v = 0; v < VW; ++v)
-                    st_row(ym, (size_t)(y0 + r) * d.ldy + j0 + v, acc[v].value(), alpha, beta);
+                    st_row(ym, (size_t)(y0 + r) * d.ldy + j0 + v, acc.value(v), alpha, beta);
             }
-#pragma unroll
-            for (int v = 0; v < VW; ++v) acc[v].zero();
+            acc.zero();
         };
 
         // ---- walk: chunks of CH nonzeros, the next chunk's x rows in flight
@@ -258,8 +334,7 @@ struct SpmmTile {
                         next_end = ly < ly_end ? row_end(s_rp, rpo, ly, x0) : INT_MAX;
                     }
                     const P av = to_p(vv[t]);
-#pragma unroll
-                    for (int v = 0; v < VW; ++v) acc[v].add(av * (P)xr[t][v]);
+                    acc.add(av, xr[t]);
                     if (DV) {
                         if (y0 + ly != xrow_of) {  // uniform within the group
                             xrow_of = y0 + ly;
@@ -295,7 +370,7 @@ struct SpmmTile {
         int f = first_row >= 0;
         double sv[VW];
 #pragma unroll
-        for (int v = 0; v < VW; ++v) sv[v] = acc[v].value();
+        for (int v = 0; v < VW; ++v) sv[v] = acc.value(v);
 #pragma unroll
         for (int o = 1; o < G; o <<= 1) {
             double t[VW];
