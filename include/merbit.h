@@ -53,7 +53,7 @@ typedef enum merbit_status {
     MERBIT_ERR_CUDA = 4,        /* a CUDA runtime call failed: merbit_last_cuda_error() */
     MERBIT_ERR_TIMEOUT = 5,     /* a device-side carry wait ran out (bounded spin); the
                                    launch's output is invalid; reported by merbit_plan_check */
-    MERBIT_ERR_UNSUPPORTED = 6  /* valid request this build does not implement */
+    MERBIT_ERR_UNSUPPORTED = 6  /* valid request the library does not implement */
 } merbit_status;
 
 typedef enum merbit_dtype {

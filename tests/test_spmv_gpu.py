@@ -3,7 +3,7 @@
 Tolerances (component-wise, e_i = |y_i - y*_i| / sum_j |a_ij x_j| against
 the extended-precision oracle computed on the stored values):
   * f64 (plain form):            1e-13
-  * f32 / bf16 (precision form): 1e-6   (the target north_star states)
+  * f32 / bf16 (precision form): 1e-6   (the precision target)
 and against the reference merbit_kernel (oracle/_ref, its own float atomics):
   * f64: 1e-12,  f32: 1e-5 (the reference accumulates in plain float)
 """
