@@ -231,10 +231,33 @@ def test_alternating_kernels_share_carry_slots(dtype):
     cfgs = plan.configs()
     warp = [c[0] for c in cfgs if c[1] == 1]
     cta = [c[0] for c in cfgs if c[1] == 0]
-    order = [warp[0], cta[0], warp[0], warp[1], cta[1], cta[0], warp[0], warp[-1], cta[-1], warp[0]]
+    rows = [c[0] for c in cfgs if c[1] == 3]
+    order = [warp[0], cta[0], warp[0], rows[0], warp[1], cta[1], cta[0], rows[-1], warp[0],
+             warp[-1], cta[-1], rows[1], warp[0]]
     for idx in order * 2:
         plan.set_config(idx)
         y = plan.spmv(xd)
         torch.cuda.synchronize()
         assert O.rel_error(y.cpu().numpy(), yo, ya)[0] <= TOL[dtype], idx
+    plan.check()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("name,A", CASES, ids=[c[0] for c in CASES])
+def test_row_groups_edge_cases(name, A, dtype):
+    """Every row-group configuration (2-32 lanes per row, both gather hints)
+    on the edge cases: empty rows, a 100k-entry row, ragged tails."""
+    x = _x(A, dtype)
+    yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+    rp, col, v = to_cuda(A, dtype)
+    plan = mb.Plan(rp, col, v, ncol=A.ncol)
+    xd = torch.from_numpy(x).cuda()
+    rows = [c for c in plan.configs() if c[1] == 3]
+    assert len(rows) >= 5
+    for idx, _, _, lpr in rows:
+        plan.set_config(idx)
+        y = plan.spmv(xd).cpu().numpy()
+        assert O.rel_error(y, yo, ya)[0] <= TOL[dtype], (idx, lpr)
+        assert np.all(y[np.diff(A.row_ptr) == 0] == 0)
     plan.check()
