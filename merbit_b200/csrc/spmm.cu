@@ -86,6 +86,7 @@ __device__ __forceinline__ unsigned long long dbits(double v) {
 // The VW accumulators of one lane.  Generic: one Acc per column.
 template <class Acc, int VW, typename P, typename X>
 struct AccRow {
+    static constexpr bool kPairs = false;
     Acc a[VW];
     __device__ __forceinline__ void zero() {
 #pragma unroll
@@ -96,6 +97,10 @@ struct AccRow {
         for (int v = 0; v < VW; ++v) a[v].add(av * (P)x[v]);
     }
     __device__ __forceinline__ double value(int v) const { return a[v].value(); }
+    __device__ __forceinline__ void add_pair(P a0, const X (&x0)[VW], P a1, const X (&x1)[VW]) {
+        add(a0, x0);
+        add(a1, x1);
+    }
 };
 
 // TwoSum accumulators of an even number of columns, two columns per packed
@@ -121,6 +126,12 @@ __device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsig
     asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
     return r;
 }
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
 __device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
     unsigned long long r;
     asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
@@ -129,6 +140,9 @@ __device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsig
 template <int VW>
 struct AccRow<AccTwoSum, VW, float, float> {
     static_assert(VW % 2 == 0, "packed TwoSum needs an even width");
+    // two products of one row may enter as their fused sum: the pair's
+    // rounding (one unit of |a0 x0| + |a1 x1|) replaces the product's
+    static constexpr bool kPairs = true;
     unsigned long long s[VW / 2], c[VW / 2];
     __device__ __forceinline__ void zero() {
 #pragma unroll
@@ -137,14 +151,24 @@ struct AccRow<AccTwoSum, VW, float, float> {
     __device__ __forceinline__ void add(float av, const float (&x)[VW]) {
         const unsigned long long a2 = f2_pack(av, av);
 #pragma unroll
+        for (int h = 0; h < VW / 2; ++h) sum(h, f2_mul(a2, f2_pack(x[2 * h], x[2 * h + 1])));
+    }
+    __device__ __forceinline__ void add_pair(float a0, const float (&x0)[VW], float a1,
+                                             const float (&x1)[VW]) {
+        const unsigned long long b0 = f2_pack(a0, a0), b1 = f2_pack(a1, a1);
+#pragma unroll
         for (int h = 0; h < VW / 2; ++h) {
-            const unsigned long long p = f2_mul(a2, f2_pack(x[2 * h], x[2 * h + 1]));
-            const unsigned long long t = f2_add(s[h], p);
-            const unsigned long long bp = f2_sub(t, s[h]);
-            const unsigned long long e = f2_add(f2_sub(s[h], f2_sub(t, bp)), f2_sub(p, bp));
-            s[h] = t;
-            c[h] = f2_add(c[h], e);
+            const unsigned long long p0 = f2_mul(b0, f2_pack(x0[2 * h], x0[2 * h + 1]));
+            sum(h, f2_fma(b1, f2_pack(x1[2 * h], x1[2 * h + 1]), p0));
         }
+    }
+    // TwoSum of p into (s[h], c[h])
+    __device__ __forceinline__ void sum(int h, unsigned long long p) {
+        const unsigned long long t = f2_add(s[h], p);
+        const unsigned long long bp = f2_sub(t, s[h]);
+        const unsigned long long e = f2_add(f2_sub(s[h], f2_sub(t, bp)), f2_sub(p, bp));
+        s[h] = t;
+        c[h] = f2_add(c[h], e);
     }
     __device__ __forceinline__ double value(int v) const {
         float s0, s1, c0, c1;
@@ -155,10 +179,16 @@ struct AccRow<AccTwoSum, VW, float, float> {
 };
 template <>
 struct AccRow<AccTwoSum, 1, float, float> {
+    static constexpr bool kPairs = false;
     AccTwoSum a;
     __device__ __forceinline__ void zero() { a.zero(); }
     __device__ __forceinline__ void add(float av, const float (&x)[1]) { a.add(av * x[0]); }
     __device__ __forceinline__ double value(int) const { return a.value(); }
+    __device__ __forceinline__ void add_pair(float a0, const float (&x0)[1], float a1,
+                                             const float (&x1)[1]) {
+        add(a0, x0);
+        add(a1, x1);
+    }
 };
 
 // DV: also form dL/dval for each nonzero (SpmmLaunch::dv_*), from the x row
@@ -281,6 +311,7 @@ struct SpmmTile {
 
         AccRow<Acc, VW, P, X> acc;
         acc.zero();
+        constexpr bool AccPairs = AccRow<Acc, VW, P, X>::kPairs;
         int first_row = -1;
         double first_val[VW];
 #pragma unroll
@@ -323,33 +354,59 @@ struct SpmmTile {
         int xrow_of = -1;
         const int* s_perm = reinterpret_cast<const int*>(ws + perm_offset);
         const unsigned gmask = LPG == 32 ? 0xFFFFFFFFu : (((1u << LPG) - 1u) << (g * LPG));
+        auto dv_step = [&](int t, int e, const X (&xr)[CH][VW]) {
+            if (y0 + ly != xrow_of) {  // uniform within the group
+                xrow_of = y0 + ly;
+                ld_vec<VW>(dvx + (size_t)xrow_of * a.dv_ldx + j0, xrow);
+            }
+            // in the x type: VW fused multiply-adds per lane, then a tree
+            // over the group's lanes (error within (VW + log2 LPG) roundings
+            // of sum |g x|)
+            X dd = (X)0;
+#pragma unroll
+            for (int v = 0; v < VW; ++v) dd = fma(xr[t][v], xrow[v], dd);
+#pragma unroll
+            for (int o = LPG / 2; o > 0; o >>= 1) dd += __shfl_xor_sync(gmask, dd, o);
+            if (jl == 0) dvo[s_perm[col_o + e]] = dd;
+        };
+        auto end_rows = [&](int e) {
+            while (next_end <= e) {
+                emit(ly);
+                ++ly;
+                next_end = ly < ly_end ? row_end(s_rp, rpo, ly, x0) : INT_MAX;
+            }
+        };
         auto consume = [&](int c, const X (&xr)[CH][VW], const V (&vv)[CH]) {
+            if (AccPairs && CH == 2) {
+                // two nonzeros of one row: one compensated addition of their
+                // fused pair sum (fma(a1, x1, a0 x0)) instead of two
+                if (c < lx_end) {
+                    end_rows(c);
+                    if (c + 1 < lx_end && next_end > c + 1) {
+                        acc.add_pair(to_p(vv[0]), xr[0], to_p(vv[1]), xr[1 % CH]);
+                        if (DV) {
+                            dv_step(0, c, xr);
+                            dv_step(1 % CH, c + 1, xr);
+                        }
+                        return;
+                    }
+                    acc.add(to_p(vv[0]), xr[0]);
+                    if (DV) dv_step(0, c, xr);
+                    if (c + 1 < lx_end) {
+                        end_rows(c + 1);
+                        acc.add(to_p(vv[1 % CH]), xr[1 % CH]);
+                        if (DV) dv_step(1 % CH, c + 1, xr);
+                    }
+                }
+                return;
+            }
 #pragma unroll
             for (int t = 0; t < CH; ++t) {
                 const int e = c + t;
                 if (e < lx_end) {
-                    while (next_end <= e) {
-                        emit(ly);
-                        ++ly;
-                        next_end = ly < ly_end ? row_end(s_rp, rpo, ly, x0) : INT_MAX;
-                    }
-                    const P av = to_p(vv[t]);
-                    acc.add(av, xr[t]);
-                    if (DV) {
-                        if (y0 + ly != xrow_of) {  // uniform within the group
-                            xrow_of = y0 + ly;
-                            ld_vec<VW>(dvx + (size_t)xrow_of * a.dv_ldx + j0, xrow);
-                        }
-                        // in the x type: VW fused multiply-adds per lane, then a
-                        // tree over the group's lanes (error within
-                        // (VW + log2 LPG) roundings of sum |g x|)
-                        X dd = (X)0;
-#pragma unroll
-                        for (int v = 0; v < VW; ++v) dd = fma(xr[t][v], xrow[v], dd);
-#pragma unroll
-                        for (int o = LPG / 2; o > 0; o >>= 1) dd += __shfl_xor_sync(gmask, dd, o);
-                        if (jl == 0) dvo[s_perm[col_o + e]] = dd;
-                    }
+                    end_rows(e);
+                    acc.add(to_p(vv[t]), xr[t]);
+                    if (DV) dv_step(t, e, xr);
                 }
             }
         };
