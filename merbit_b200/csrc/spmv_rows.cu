@@ -4,7 +4,7 @@
 // path walk costs more than it saves: every item goes through shared memory
 // twice and every row end through a scan.  Here a group of LPR lanes owns a
 // whole row: the lanes read the row's col_idx/vals coalesced (lane j takes
-// nonzeros j, j+LPR, ...), keep up to 8 gathers of x in flight, accumulate with
+// nonzeros j, j+LPR, ...), keep 4-16 gathers of x in flight, accumulate with
 // the dtype's policy (F64: double; F32/BF16: TwoSum), and the group combines
 // its lane sums by a fixed butterfly in double.  No row spans two groups, so
 // there are no carries, no atomics and no shared memory; results are
