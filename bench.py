@@ -296,9 +296,18 @@ def run_ours(args):
     xd = torch.from_numpy(x).to(dev).to(xt)
     yd = torch.empty(A.nrow, dtype=xt, device=dev)
     torch.cuda.synchronize(dev)
+    # plan build, as the reference's tim1 times its TILE build
+    # (include/tile.cuh:587-593): CUDA events on the stream around it, and
+    # the host wall time (allocation and synchronization included)
+    ev_p0 = torch.cuda.Event(enable_timing=True)
+    ev_p1 = torch.cuda.Event(enable_timing=True)
+    ev_p0.record(torch.cuda.current_stream(dev))
     t_plan0 = time.perf_counter()
     plan = mb.Plan(rp, col, vals, ncol=A.ncol)  # validates, partitions; synchronizes
     t_plan = time.perf_counter() - t_plan0
+    ev_p1.record(torch.cuda.current_stream(dev))
+    torch.cuda.synchronize(dev)
+    t_plan_ev = ev_p0.elapsed_time(ev_p1)
     if args.config >= 0:
         plan.set_config(args.config)
     elif not args.no_tune:
@@ -443,6 +452,7 @@ def run_ours(args):
         "algorithmic_bytes_per_step": B,
         "plan_metadata_bytes": info.metadata_bytes,
         "plan_build_ms_host_wall": round(t_plan * 1e3, 3),
+        "plan_build_ms_events": round(t_plan_ev, 3),
         "gpu_launches": args.steps,
         "roofline": {
             "bound": "hbm",
