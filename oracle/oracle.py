@@ -11,6 +11,10 @@ never by the ``merbit_b200`` package.
 * ``ref()`` -> oracle/_ref/libmerbit_ref.so (oracle/ref_harness.cu): the
   reference's own merge_search / Tile_Kernel / merbit_kernel, compiled from
   the reference sources by oracle/Makefile.  ``None`` when not built.
+* ``comp()`` -> oracle/_ref/libmerbit_competitors.so (oracle/competitors.cu):
+  the libraries the reference compares against (cuSPARSE CSR_ALG2 / COO_ALG2,
+  CUB DeviceSpmv, vendored CSR5 and HOLA), timed as src/spmv.cu calls them.
+  ``None`` when not built.
 """
 from __future__ import annotations
 
@@ -23,6 +27,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libmerbit_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmerbit_ref.so")
+COMP_SO = os.path.join(HERE, "_ref", "libmerbit_competitors.so")
 
 F64, F32, BF16 = 0, 1, 2
 _i64 = C.c_int64
@@ -31,6 +36,8 @@ _p = C.c_void_p
 _lib = None
 _ref = None
 _ref_tried = False
+_comp = None
+_comp_tried = False
 
 
 def build() -> None:
@@ -84,6 +91,27 @@ def ref():
             R.ref_merbit_time_sigma.restype = C.c_float
             _ref = R
     return _ref
+
+
+def comp():
+    """The competitor-library harness, or None when oracle/_ref was not built.
+    Every entry returns 0 or an error code; times are mean ms per call."""
+    global _comp, _comp_tried
+    if not _comp_tried:
+        _comp_tried = True
+        if os.path.exists(COMP_SO):
+            L = C.CDLL(COMP_SO)
+            f = C.POINTER(C.c_float)
+            i = C.POINTER(C.c_int)
+            L.comp_cusparse_time.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _p, _p, _p, _p,
+                                             _p, _p, C.c_int, f]
+            L.comp_cub_time.argtypes = [C.c_int, C.c_int, C.c_int, _p, _p, _p, _p, _p, C.c_int, f]
+            L.comp_csr5_time.argtypes = [C.c_int, C.c_int, C.c_int, _p, _p, _p, _p, _p, C.c_int,
+                                         f, f, i]
+            L.comp_hola_time.argtypes = [C.c_int, C.c_int, C.c_int, _p, _p, _p, _p, _p, C.c_int,
+                                         f, f]
+            _comp = L
+    return _comp
 
 
 def _ptr(a: np.ndarray):
