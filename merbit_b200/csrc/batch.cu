@@ -15,8 +15,13 @@ int alloc_spmm_slots(SpmmSlots* s, long long nslots, cudaStream_t st) {
     if (nslots <= 0) nslots = 1;
     if (nslots > INT_MAX) return fail(MERBIT_ERR_OVERFLOW, "spmm: tiles * k exceeds int32");
     const size_t words = 4 * (size_t)nslots;
-    MERBIT_CUDA(cudaMalloc(&s->words, sizeof(unsigned long long) * words));
-    MERBIT_CUDA(cudaMalloc(&s->state, sizeof(LaunchState)));
+    int rc = dev_alloc(&s->words, sizeof(unsigned long long) * words, st);
+    if (rc == MERBIT_OK) rc = dev_alloc(&s->state, sizeof(LaunchState), st);
+    if (rc != MERBIT_OK) {
+        dev_free(s->words, st);
+        s->words = nullptr;
+        return rc;
+    }
     MERBIT_CUDA(cudaMemsetAsync(s->words, 0xFF, sizeof(unsigned long long) * words, st));
     LaunchState init = {};
     init.epoch = 1u;
@@ -123,6 +128,7 @@ int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long 
 // Batch of plans sharing one persistent launch.
 struct merbit_batch_s {
     int count = 0, k = 0, dtype = 0, items = 256, vw = 1;
+    int device = 0;
     std::vector<merbit_plan_s*> plans;
     std::vector<const void*> x;
     std::vector<void*> y;
@@ -154,12 +160,16 @@ int batch_build(merbit_batch_s* b, int items, cudaStream_t s) {
     for (int i = 0; i < b->count; ++i)
         vw = std::min(vw, pick_vw(b->k, b->ldx[i], b->x[i], b->y[i], b->ldy[i], esz, items));
     if (!spmm_config_exists(b->k, vw, items)) vw = 1;
-    if (b->d_descs == nullptr) MERBIT_CUDA(cudaMalloc(&b->d_descs, sizeof(SpmmDesc) * b->count));
+    if (b->d_descs == nullptr) {
+        int st = dev_alloc(&b->d_descs, sizeof(SpmmDesc) * b->count, s);
+        if (st != MERBIT_OK) return st;
+    }
     MERBIT_CUDA(cudaMemcpyAsync(b->d_descs, h.data(), sizeof(SpmmDesc) * b->count,
                                 cudaMemcpyHostToDevice, s));
     if (b->slots.nslots < tot * b->k) {
-        cudaFree(b->slots.words);
-        cudaFree(b->slots.state);
+        if (b->slots.words) MERBIT_CUDA(cudaDeviceSynchronize());  // launches may use them
+        dev_free(b->slots.words, s);
+        dev_free(b->slots.state, s);
         b->slots = SpmmSlots();
         int st = alloc_spmm_slots(&b->slots, tot * b->k, s);
         if (st != MERBIT_OK) return st;
@@ -241,6 +251,7 @@ int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* p
         return fail(MERBIT_ERR_INVALID, "batch_create: bad arguments");
     if (!pow2(k) || k > 32) return fail(MERBIT_ERR_UNSUPPORTED, "batch_create: k must be 1, 2, 4, 8, 16 or 32");
     auto* b = new merbit_batch_s();
+    cudaGetDevice(&b->device);
     b->count = count;
     b->k = k;
     b->dtype = plans[0] ? plans[0]->dtype : 0;
@@ -334,9 +345,15 @@ int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info) {
 
 int merbit_batch_destroy(merbit_batch batch) {
     if (!batch) return MERBIT_OK;
-    cudaFree(batch->d_descs);
-    cudaFree(batch->slots.words);
-    cudaFree(batch->slots.state);
+    // wait for the batch's launches, as cudaFree does, then release
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != batch->device) cudaSetDevice(batch->device);
+    cudaDeviceSynchronize();
+    dev_free(batch->d_descs, nullptr);
+    dev_free(batch->slots.words, nullptr);
+    dev_free(batch->slots.state, nullptr);
+    if (cur != batch->device) cudaSetDevice(cur);
     delete batch;
     return MERBIT_OK;
 }

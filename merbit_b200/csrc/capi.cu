@@ -32,37 +32,72 @@ int cuda_fail(cudaError_t e, const char* where) {
     return MERBIT_ERR_CUDA;
 }
 
-int validate_csr(const int32_t* row_ptr, const int32_t* col, int nrow, int ncol, int nnz,
-                 cudaStream_t s);
 
 namespace {
+
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Grows the plan's carry slots to `tiles` (both parity arrays start empty:
+// all ones).  The fill is ordered on s; callers synchronize s before a
+// launch on another stream can use the slots.
+int grow_carry(merbit_plan_s* p, int tiles, cudaStream_t s) {
+    if (tiles <= p->slots) return MERBIT_OK;
+    if (p->carry) {  // launches in flight may still use the old slots
+        MERBIT_CUDA(cudaDeviceSynchronize());
+        dev_free(p->carry, s);
+        p->carry = nullptr;
+        p->slots = 0;
+    }
+    const size_t words = 4 * (size_t)tiles;  // carries + boundary swaps, 2 parities
+    int st = dev_alloc(&p->carry, sizeof(unsigned long long) * words, s);
+    if (st != MERBIT_OK) return st;
+    MERBIT_CUDA(cudaMemsetAsync(p->carry, 0xFF, sizeof(unsigned long long) * words, s));
+    p->slots = tiles;
+    return MERBIT_OK;
+}
+
+// Starts a partition for `tile_items` without synchronizing; its largest
+// rows-per-tile lands in p->scratch->max_rows for the caller's next
+// readback.  On failure nothing is added to the plan.
+int plan_partition_start(merbit_plan_s* p, int tile_items, Partition** out, cudaStream_t s) {
+    MERBIT_CUDA(cudaMemsetAsync(&p->scratch->max_rows, 0, sizeof(int), s));
+    Partition q;
+    int st = build_partition_async(p->row_ptr, p->nrow, p->nnz, tile_items, &q,
+                                   &p->scratch->max_rows, s);
+    if (st == MERBIT_OK) st = grow_carry(p, q.num_tiles, s);
+    if (st != MERBIT_OK) {
+        dev_free(q.coords, s);
+        return st;
+    }
+    p->parts.push_back(q);
+    *out = &p->parts.back();
+    return MERBIT_OK;
+}
+
 }  // namespace
 
 // Ensures the plan holds a partition for `tile_items` and enough carry
-// slots; returns it in *out.
+// slots; returns it in *out.  Synchronizes s when it builds one.
 int plan_partition(merbit_plan_s* p, int tile_items, const Partition** out, cudaStream_t s) {
     for (auto& q : p->parts)
         if (q.tile_items == tile_items) {
             *out = &q;
             return MERBIT_OK;
         }
-    Partition q;
-    int st = build_partition(p->row_ptr, p->nrow, p->nnz, tile_items, &q, s);
+    Partition* q = nullptr;
+    int st = plan_partition_start(p, tile_items, &q, s);
     if (st != MERBIT_OK) return st;
-    if (q.num_tiles > p->slots) {
-        // grow the carry slots: both parity arrays start empty (all ones)
-        MERBIT_CUDA(cudaStreamSynchronize(s));
-        cudaFree(p->carry);
-        p->carry = nullptr;
-        const size_t words = 4 * (size_t)q.num_tiles;  // carries + boundary swaps, 2 parities
-        MERBIT_CUDA(cudaMalloc(&p->carry, sizeof(unsigned long long) * words));
-        MERBIT_CUDA(cudaMemsetAsync(p->carry, 0xFF, sizeof(unsigned long long) * words, s));
-        MERBIT_CUDA(cudaStreamSynchronize(s));
-        p->slots = q.num_tiles;
+    int h_max = 0;
+    cudaError_t e = cudaMemcpyAsync(&h_max, &p->scratch->max_rows, sizeof(int),
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        dev_free(q->coords, s);
+        p->parts.pop_back();
+        return cuda_fail(e, "partition: max rows");
     }
-    p->parts.push_back(q);
-    *out = &p->parts.back();
+    q->max_rows = h_max;
+    *out = q;
     return MERBIT_OK;
 }
 
@@ -102,15 +137,16 @@ int plan_pick_default(merbit_plan_s* p, cudaStream_t s) {
 // Grows the plan's residual partials to hold one word per CTA of any launch
 // over `num_tiles` tiles (warp-tile kernel: at most 32 resident CTAs per SM;
 // CTA-tile kernel: one CTA per tile).
-int plan_partials(merbit_plan_s* p, int num_tiles) {
+int plan_partials(merbit_plan_s* p, int num_tiles, cudaStream_t s) {
     int sms = 0;
     MERBIT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
     const long long need = std::max<long long>(num_tiles, 32LL * std::max(sms, 1));
     if (need <= p->npartials) return MERBIT_OK;
-    cudaFree(p->partials);
+    dev_free(p->partials, s);  // ordered after this plan's earlier launches
     p->partials = nullptr;
     p->npartials = 0;
-    MERBIT_CUDA(cudaMalloc(&p->partials, sizeof(double) * (size_t)need));
+    int st = dev_alloc(&p->partials, sizeof(double) * (size_t)need, s);
+    if (st != MERBIT_OK) return st;
     p->npartials = need;
     return MERBIT_OK;
 }
@@ -127,7 +163,7 @@ int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta
         if (st != MERBIT_OK) return st;
     }
     if (residual) {
-        st = plan_partials(p, part ? part->num_tiles : 0);
+        st = plan_partials(p, part ? part->num_tiles : 0, s);
         if (st != MERBIT_OK) return st;
     }
     SpmvLaunch a;
@@ -224,10 +260,6 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
     if ((long long)nrow + nnz > (long long)INT_MAX - 64)
         return fail(MERBIT_ERR_OVERFLOW, "plan_create: nrow+nnz exceeds the int32 merge-path range");
     cudaStream_t s = (cudaStream_t)stream;
-    if (!(flags & MERBIT_PLAN_SKIP_VALIDATE)) {
-        int st = validate_csr(d_row_ptr, d_col_idx, nrow, ncol, nnz, s);
-        if (st != MERBIT_OK) return st;
-    }
     auto* p = new merbit_plan_s();
     p->nrow = nrow;
     p->ncol = ncol;
@@ -244,30 +276,55 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
         auto it = g_tune.find(signature(p));
         if (it != g_tune.end()) tuned = it->second;
     }
-    cudaError_t e = cudaMalloc(&p->state, sizeof(LaunchState));
-    if (e != cudaSuccess) {
+    // one allocation for the launch state and the build's readback words;
+    // the whole build (validation, first partition, carry slots) is queued
+    // on s and read back with one synchronization
+    static_assert(sizeof(LaunchState) % alignof(PlanScratch) == 0, "scratch alignment");
+    int st = dev_alloc(&p->state, sizeof(LaunchState) + sizeof(PlanScratch), s);
+    if (st != MERBIT_OK) {
         delete p;
-        return cuda_fail(e, "plan_create: cudaMalloc(state)");
+        return st;
     }
-    LaunchState init = {};
-    init.epoch = 1u;
-    e = cudaMemcpyAsync(p->state, &init, sizeof(init), cudaMemcpyHostToDevice, s);
+    p->scratch = reinterpret_cast<PlanScratch*>(p->state + 1);
+    struct {
+        LaunchState ls;
+        PlanScratch sc;
+    } init = {};
+    static_assert(sizeof(init) == sizeof(LaunchState) + sizeof(PlanScratch), "state layout");
+    init.ls.epoch = 1u;
+    init.sc = PlanScratch{0, {INT_MAX, INT_MAX}, 0};
+    cudaError_t e = cudaMemcpyAsync(p->state, &init, sizeof(init), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
         merbit_plan_destroy(p);
         return cuda_fail(e, "plan_create: init state");
     }
-    int st = MERBIT_OK;
-    bool tuned_ok = false;
-    if (tuned >= 0) st = plan_config_ok(p, tuned, &tuned_ok, s);
+    const bool validate = !(flags & MERBIT_PLAN_SKIP_VALIDATE);
+    st = validate ? validate_launch(d_row_ptr, d_col_idx, nrow, ncol, nnz, p->scratch, s)
+                  : MERBIT_OK;
+    // first candidate: the configuration tuned for this matrix signature,
+    // else the table's first entry the plan's alignment allows
+    int first = -1;
+    if (tuned >= 0 && spmv_config_allowed(spmv_config(dtype, tuned), p->vec)) first = tuned;
+    for (int i = 0, n = spmv_num_configs(dtype); first < 0 && i < n; ++i)
+        if (spmv_config_allowed(spmv_config(dtype, i), p->vec)) first = i;
+    Partition* part = nullptr;
+    if (st == MERBIT_OK && first >= 0 && spmv_config(dtype, first).kind != 3)
+        st = plan_partition_start(p, spmv_tile_items(spmv_config(dtype, first)), &part, s);
+    PlanScratch h = {};
     if (st == MERBIT_OK) {
-        if (tuned_ok)
-            p->cfg = tuned;
-        else
-            st = plan_pick_default(p, s);
+        e = cudaMemcpyAsync(&h, p->scratch, sizeof(h), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(e, "plan_create: readback");
     }
+    if (st == MERBIT_OK && validate) st = validate_status(h);
     if (st == MERBIT_OK) {
-        e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) st = cuda_fail(e, "plan_create: sync");
+        if (part) part->max_rows = h.max_rows;
+        const bool ok = first >= 0 && (!part || h.max_rows <= spmv_config_row_cap(
+                                                                   spmv_config(dtype, first)));
+        if (ok)
+            p->cfg = first;
+        else
+            st = plan_pick_default(p, s);  // reuses the partition built above
     }
     if (st != MERBIT_OK) {
         merbit_plan_destroy(p);
@@ -279,16 +336,23 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
 
 int merbit_plan_destroy(merbit_plan plan) {
     if (!plan) return MERBIT_OK;
-    for (auto& q : plan->parts) cudaFree(q.coords);
+    // the plan's launches may still run on any stream: wait for the device,
+    // as cudaFree does, then hand the blocks back to the pool
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != plan->device) cudaSetDevice(plan->device);
+    cudaDeviceSynchronize();
+    for (auto& q : plan->parts) dev_free(q.coords, nullptr);
     for (auto& kv : plan->spmm_slots) {
-        cudaFree(kv.second.words);
-        cudaFree(kv.second.state);
+        dev_free(kv.second.words, nullptr);
+        dev_free(kv.second.state, nullptr);
     }
-    cudaFree(plan->carry);
-    cudaFree(plan->state);
-    cudaFree(plan->row_of);
-    cudaFree(plan->partials);
-    for (void* q : plan->owned) cudaFree(q);
+    dev_free(plan->carry, nullptr);
+    dev_free(plan->state, nullptr);
+    dev_free(plan->row_of, nullptr);
+    dev_free(plan->partials, nullptr);
+    for (void* q : plan->owned) dev_free(q, nullptr);
+    if (cur != plan->device) cudaSetDevice(cur);
     delete plan;
     return MERBIT_OK;
 }

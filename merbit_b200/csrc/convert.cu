@@ -90,13 +90,13 @@ int merbit_coo_sort(int32_t nnz, int32_t* d_major, int32_t* d_minor, void* d_val
     void* tmpv = nullptr;
     void* temp = nullptr;
     const size_t vs = dtype_size(dtype);
-    auto done = [&](int st) {
-        cudaFree(k_in);
-        cudaFree(k_out);
-        cudaFree(i_in);
-        cudaFree(i_out);
-        cudaFree(tmpv);
-        cudaFree(temp);
+    auto done = [&](int st) {  // stream-ordered: after the sort's own work on s
+        dev_free(k_in, s);
+        dev_free(k_out, s);
+        dev_free(i_in, s);
+        dev_free(i_out, s);
+        dev_free(tmpv, s);
+        dev_free(temp, s);
         return st;
     };
 #define TRY(call)                                              \
@@ -104,18 +104,23 @@ int merbit_coo_sort(int32_t nnz, int32_t* d_major, int32_t* d_minor, void* d_val
         cudaError_t _e = (call);                               \
         if (_e != cudaSuccess) return done(cuda_fail(_e, #call)); \
     } while (0)
-    TRY(cudaMalloc(&k_in, 8 * (size_t)nnz));
-    TRY(cudaMalloc(&k_out, 8 * (size_t)nnz));
-    TRY(cudaMalloc(&i_in, 4 * (size_t)nnz));
-    TRY(cudaMalloc(&i_out, 4 * (size_t)nnz));
+#define TRY_ALLOC(p, bytes)                              \
+    do {                                                 \
+        int _st = dev_alloc(&(p), (bytes), s);           \
+        if (_st != MERBIT_OK) return done(_st);          \
+    } while (0)
+    TRY_ALLOC(k_in, 8 * (size_t)nnz);
+    TRY_ALLOC(k_out, 8 * (size_t)nnz);
+    TRY_ALLOC(i_in, 4 * (size_t)nnz);
+    TRY_ALLOC(i_out, 4 * (size_t)nnz);
     pack_keys<<<grid_of(nnz), 256, 0, s>>>(d_major, d_minor, nnz, k_in, i_in);
     size_t tb = 0;
     TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, k_in, k_out, i_in, i_out, nnz, 0, 64, s));
-    TRY(cudaMalloc(&temp, tb));
+    TRY_ALLOC(temp, tb);
     TRY(cub::DeviceRadixSort::SortPairs(temp, tb, k_in, k_out, i_in, i_out, nnz, 0, 64, s));
     unpack_keys<<<grid_of(nnz), 256, 0, s>>>(k_out, nnz, d_major, d_minor);
     if (d_vals) {
-        TRY(cudaMalloc(&tmpv, vs * (size_t)nnz));
+        TRY_ALLOC(tmpv, vs * (size_t)nnz);
         TRY(cudaMemcpyAsync(tmpv, d_vals, vs * (size_t)nnz, cudaMemcpyDeviceToDevice, s));
         if (dtype == MERBIT_F64)
             permute_vals<double><<<grid_of(nnz), 256, 0, s>>>((const double*)tmpv, i_out, nnz,
@@ -130,6 +135,7 @@ int merbit_coo_sort(int32_t nnz, int32_t* d_major, int32_t* d_minor, void* d_val
     TRY(cudaGetLastError());
     TRY(cudaStreamSynchronize(s));
 #undef TRY
+#undef TRY_ALLOC
     return done(MERBIT_OK);
 }
 
@@ -151,7 +157,8 @@ int merbit_outdegree_values(int32_t nnz, int32_t nrow, const int32_t* d_row_ind,
     cudaStream_t s = (cudaStream_t)stream;
     int* cnt = nullptr;
     const size_t cbytes = sizeof(int) * ((size_t)nrow + 1);
-    MERBIT_CUDA(cudaMalloc(&cnt, cbytes));
+    int st = dev_alloc(&cnt, cbytes, s);
+    if (st != MERBIT_OK) return st;
     int bad = 0;
     cudaError_t e = cudaMemsetAsync(cnt, 0, cbytes, s);
     if (e == cudaSuccess) {
@@ -170,7 +177,7 @@ int merbit_outdegree_values(int32_t nnz, int32_t nrow, const int32_t* d_row_ind,
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(&bad, cnt + nrow, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(cnt);
+    dev_free(cnt, s);
     if (e != cudaSuccess) return cuda_fail(e, "outdegree_values");
     if (bad) return fail(MERBIT_ERR_MATRIX, "outdegree_values: row index outside [0, nrow)");
     return MERBIT_OK;

@@ -331,6 +331,18 @@ int cuda_fail(cudaError_t e, const char* where);
         if (_e != cudaSuccess) return ::merbit::cuda_fail(_e, #call); \
     } while (0)
 
+// Device memory (pool.cu): stream-ordered blocks from one pool per device
+// that keeps released blocks mapped.  dev_alloc allocates on the current
+// device, ordered on s; dev_free releases in order on s.  An owner released
+// without a stream (plan or batch destroy) synchronizes the device first,
+// as cudaFree would, and frees on the legacy stream.
+int dev_alloc(void** p, size_t bytes, cudaStream_t s);
+void dev_free(void* p, cudaStream_t s);
+template <class T>
+int dev_alloc(T** p, size_t bytes, cudaStream_t s) {
+    return dev_alloc(reinterpret_cast<void**>(p), bytes, s);
+}
+
 inline size_t dtype_size(int dt) { return dt == MERBIT_F64 ? 8 : dt == MERBIT_F32 ? 4 : 2; }
 inline size_t xy_size(int dt) { return dt == MERBIT_F64 ? 8 : 4; }
 
@@ -348,8 +360,27 @@ struct Partition {
 // cannot use that configuration.
 constexpr int warp_rp_cap(int ipt) { return (32 * ipt) / 3 + 16; }
 
-int build_partition(const int32_t* row_ptr, int nrow, int nnz, int tile_items, Partition* out,
-                    cudaStream_t s);
+// Allocates out->coords and queues the merge-path search of every tile
+// boundary on s, without synchronizing; the largest rows-per-tile is
+// atomically maxed into *d_max_rows (zeroed by the caller), and
+// out->max_rows stays -1 until the caller reads it back.
+int build_partition_async(const int32_t* row_ptr, int nrow, int nnz, int tile_items,
+                          Partition* out, int* d_max_rows, cudaStream_t s);
+
+// Device words a plan build reads back once: validation result (error bits,
+// first decreasing row, first bad column) and the new partition's largest
+// rows-per-tile.  Lives right after the plan's LaunchState.
+struct PlanScratch {
+    int err;
+    int first_bad[2];
+    int max_rows;
+};
+// Launches the structural CSR checks into sc->err / sc->first_bad (the
+// caller initializes them to 0 / INT_MAX); validate_status turns the words
+// read back into a status.
+int validate_launch(const int32_t* row_ptr, const int32_t* col, int nrow, int ncol, int nnz,
+                    PlanScratch* sc, cudaStream_t s);
+int validate_status(const PlanScratch& h);
 
 // Carry / swap words of one SpMM slot family (2 parities x 2 arrays x
 // tiles x k) with its own launch state.
@@ -538,6 +569,7 @@ struct merbit_plan_s {
     unsigned long long* carry = nullptr;
     int slots = 0;
     merbit::LaunchState* state = nullptr;
+    merbit::PlanScratch* scratch = nullptr;  // same allocation as state
     // SpMM carry slots, keyed by (k << 20 | tile items)
     std::map<long long, merbit::SpmmSlots> spmm_slots;
     // adjoint support: row index of every nonzero (built on first use), and

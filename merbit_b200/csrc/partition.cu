@@ -134,14 +134,16 @@ __global__ void max_rows_kernel(const int2* __restrict__ coords, int num_tiles,
     if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
-int build_partition(const int32_t* row_ptr, int nrow, int nnz, int tile_items, Partition* out,
-                    cudaStream_t s) {
+int build_partition_async(const int32_t* row_ptr, int nrow, int nnz, int tile_items,
+                          Partition* out, int* d_max_rows, cudaStream_t s) {
     const long long total = (long long)nrow + nnz;
     const long long T = (total + tile_items - 1) / tile_items;
     if (T > INT_MAX - 2) return fail(MERBIT_ERR_OVERFLOW, "partition: too many tiles");
     out->tile_items = tile_items;
     out->num_tiles = (int)T;
-    MERBIT_CUDA(cudaMalloc(&out->coords, sizeof(int2) * (size_t)(T + 1)));
+    out->max_rows = -1;
+    int st = dev_alloc(&out->coords, sizeof(int2) * (size_t)(T + 1), s);
+    if (st != MERBIT_OK) return st;
     const long long count = T + 1;
     const int bs = 256;
     const unsigned grid = (unsigned)((count + bs - 1) / bs);
@@ -149,48 +151,34 @@ int build_partition(const int32_t* row_ptr, int nrow, int nnz, int tile_items, P
                                             nullptr, out->coords);
     MERBIT_CUDA(cudaGetLastError());
     // largest rows-per-tile, which decides the configurations the plan can use
-    int* d_max = nullptr;
-    MERBIT_CUDA(cudaMalloc(&d_max, sizeof(int)));
-    int h_max = 0;
-    cudaError_t e = cudaMemsetAsync(d_max, 0, sizeof(int), s);
-    if (e == cudaSuccess && T > 0) {
+    if (T > 0) {
         max_rows_kernel<<<(unsigned)min((T + 255) / 256, 1024LL), 256, 0, s>>>(out->coords, (int)T,
-                                                                               d_max);
-        e = cudaGetLastError();
+                                                                               d_max_rows);
+        MERBIT_CUDA(cudaGetLastError());
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_max, d_max, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d_max);
-    if (e != cudaSuccess) return cuda_fail(e, "build_partition: max rows");
-    out->max_rows = h_max;
     return MERBIT_OK;
 }
 
-int validate_csr(const int32_t* row_ptr, const int32_t* col, int nrow, int ncol, int nnz,
-                 cudaStream_t s) {
-    int* d = nullptr;
-    MERBIT_CUDA(cudaMalloc(&d, 3 * sizeof(int)));
-    int h[3] = {0, INT_MAX, INT_MAX};
-    cudaError_t e = cudaMemcpyAsync(d, h, sizeof(h), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) {
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        validate_kernel<<<sms * 8, 256, 0, s>>>(row_ptr, col, nrow, ncol, nnz, d, d + 1);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d);
-    if (e != cudaSuccess) return cuda_fail(e, "validate_csr");
-    if (h[0] & 1) return fail(MERBIT_ERR_MATRIX, "row_ptr[0] != 0");
-    if (h[0] & 2) return fail(MERBIT_ERR_MATRIX, "row_ptr[nrow] != nnz");
-    if (h[0] & 4)
+int validate_launch(const int32_t* row_ptr, const int32_t* col, int nrow, int ncol, int nnz,
+                    PlanScratch* sc, cudaStream_t s) {
+    int dev = 0, sms = 148;
+    MERBIT_CUDA(cudaGetDevice(&dev));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    validate_kernel<<<sms * 8, 256, 0, s>>>(row_ptr, col, nrow, ncol, nnz, &sc->err,
+                                            sc->first_bad);
+    MERBIT_CUDA(cudaGetLastError());
+    return MERBIT_OK;
+}
+
+int validate_status(const PlanScratch& h) {
+    if (h.err & 1) return fail(MERBIT_ERR_MATRIX, "row_ptr[0] != 0");
+    if (h.err & 2) return fail(MERBIT_ERR_MATRIX, "row_ptr[nrow] != nnz");
+    if (h.err & 4)
         return fail(MERBIT_ERR_MATRIX,
-                    "row_ptr decreases after row " + std::to_string(h[1]));
-    if (h[0] & 8)
+                    "row_ptr decreases after row " + std::to_string(h.first_bad[0]));
+    if (h.err & 8)
         return fail(MERBIT_ERR_MATRIX,
-                    "column index out of range at nonzero " + std::to_string(h[2]));
+                    "column index out of range at nonzero " + std::to_string(h.first_bad[1]));
     return MERBIT_OK;
 }
 

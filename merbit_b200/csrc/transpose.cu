@@ -213,7 +213,8 @@ int launch_dval(const merbit_plan_s* p, int k, const void* g, long long ldg, con
 
 int ensure_row_of(merbit_plan_s* p, cudaStream_t s) {
     if (p->row_of || p->nnz == 0) return MERBIT_OK;
-    MERBIT_CUDA(cudaMalloc(&p->row_of, sizeof(int) * (size_t)p->nnz));
+    int st = dev_alloc(&p->row_of, sizeof(int) * (size_t)p->nnz, s);
+    if (st != MERBIT_OK) return st;
     row_of_kernel<<<grid_for(p->nnz), 256, 0, s>>>(p->row_ptr, p->nrow, p->nnz, p->row_of);
     MERBIT_CUDA(cudaGetLastError());
     return MERBIT_OK;
@@ -254,17 +255,17 @@ int merbit_plan_transpose(merbit_plan plan, merbit_plan* tplan, void* stream) {
     int* iota = nullptr;
     void* temp = nullptr;
     int st = MERBIT_OK;
-    auto cleanup = [&]() {
-        cudaFree(keys_out);
-        cudaFree(iota);
-        cudaFree(temp);
+    auto cleanup = [&]() {  // stream-ordered: after the build's work on s
+        dev_free(keys_out, s);
+        dev_free(iota, s);
+        dev_free(temp, s);
     };
     auto bail = [&](int status) {
         cleanup();
-        cudaFree(col_ptr);
-        cudaFree(row_idx);
-        cudaFree(perm);
-        cudaFree(vals_t);
+        dev_free(col_ptr, s);
+        dev_free(row_idx, s);
+        dev_free(perm, s);
+        dev_free(vals_t, s);
         return status;
     };
 #define TRY_CUDA(call)                                                  \
@@ -272,23 +273,28 @@ int merbit_plan_transpose(merbit_plan plan, merbit_plan* tplan, void* stream) {
         cudaError_t _e = (call);                                        \
         if (_e != cudaSuccess) return bail(cuda_fail(_e, #call));       \
     } while (0)
-    TRY_CUDA(cudaMalloc(&col_ptr, sizeof(int) * ((size_t)ncol + 1)));
+#define TRY_ALLOC(p, bytes)                           \
+    do {                                              \
+        int _st = dev_alloc(&(p), (bytes), s);        \
+        if (_st != MERBIT_OK) return bail(_st);       \
+    } while (0)
+    TRY_ALLOC(col_ptr, sizeof(int) * ((size_t)ncol + 1));
     const size_t nz = nnz > 0 ? (size_t)nnz : 1;
-    TRY_CUDA(cudaMalloc(&row_idx, sizeof(int) * nz));
-    TRY_CUDA(cudaMalloc(&perm, sizeof(int) * nz));
-    TRY_CUDA(cudaMalloc(&vals_t, dtype_size(plan->dtype) * nz));
+    TRY_ALLOC(row_idx, sizeof(int) * nz);
+    TRY_ALLOC(perm, sizeof(int) * nz);
+    TRY_ALLOC(vals_t, dtype_size(plan->dtype) * nz);
     st = ensure_row_of(plan, s);
     if (st != MERBIT_OK) return bail(st);
     if (nnz > 0) {
-        TRY_CUDA(cudaMalloc(&keys_out, sizeof(int) * nz));
-        TRY_CUDA(cudaMalloc(&iota, sizeof(int) * nz));
+        TRY_ALLOC(keys_out, sizeof(int) * nz);
+        TRY_ALLOC(iota, sizeof(int) * nz);
         iota_kernel<<<grid_for(nnz), 256, 0, s>>>(iota, nnz);
         int bits = 1;
         while (bits < 31 && (1ll << bits) < (long long)ncol) ++bits;
         size_t tb = 0;
         TRY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, plan->col, keys_out, iota, perm, nnz,
                                                  0, bits, s));
-        TRY_CUDA(cudaMalloc(&temp, tb));
+        TRY_ALLOC(temp, tb);
         TRY_CUDA(cub::DeviceRadixSort::SortPairs(temp, tb, plan->col, keys_out, iota, perm, nnz, 0,
                                                  bits, s));
         col_ptr_kernel<<<grid_for((long long)nnz + 1), 256, 0, s>>>(keys_out, nnz, ncol, col_ptr);
@@ -302,14 +308,15 @@ int merbit_plan_transpose(merbit_plan plan, merbit_plan* tplan, void* stream) {
     TRY_CUDA(cudaStreamSynchronize(s));
     cleanup();
 #undef TRY_CUDA
+#undef TRY_ALLOC
     merbit_plan t = nullptr;
     st = merbit_plan_create(&t, ncol, plan->nrow, nnz, col_ptr, row_idx, vals_t,
                             (merbit_dtype)plan->dtype, MERBIT_PLAN_SKIP_VALIDATE, stream);
     if (st != MERBIT_OK) {
-        cudaFree(col_ptr);
-        cudaFree(row_idx);
-        cudaFree(perm);
-        cudaFree(vals_t);
+        dev_free(col_ptr, s);
+        dev_free(row_idx, s);
+        dev_free(perm, s);
+        dev_free(vals_t, s);
         return st;
     }
     t->owned.push_back(col_ptr);

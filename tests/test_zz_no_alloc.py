@@ -58,7 +58,9 @@ def test_noalloc_matches_plan_entry_point(dtype):
         torch.cuda.synchronize()
         if call == 1:
             # after the first call's one-time set-up nothing is allocated
-            assert torch.cuda.mem_get_info()[0] == free_before
+            # (free memory can only grow: the library's memory pool may hand
+            # blocks of destroyed plans back to the device at a synchronization)
+            assert torch.cuda.mem_get_info()[0] >= free_before
         err = np.abs(y.cpu().numpy().astype(np.float64) - y_ref) / denom
         assert np.isfinite(err).all()
         assert err.max() <= TOL[dtype], (call, err.max())
