@@ -27,6 +27,7 @@
  *   merbit_plan_tune, merbit_plan_set_config   the configuration table
  *   merbit_spmv_noalloc   one SpMV that allocates nothing
  *   merbit_plan_check, merbit_plan_selftest_wait   device-side failure status
+ *   merbit_release_cached_memory   empties the library's device memory pool
  *
  * Threading: a plan may be used from any host thread, but launches that use
  * the same plan must be ordered on the device (one stream, or ordered by
@@ -276,6 +277,14 @@ int merbit_plan_check(merbit_plan plan, void* stream);
  * wait runs out, records MERBIT_ERR_TIMEOUT in the plan's device status and
  * returns; merbit_plan_check then reports it.  No fault, trap or hang. */
 int merbit_plan_selftest_wait(merbit_plan plan, int32_t which, int32_t wait_us, void* stream);
+
+/* Device memory (no reference counterpart).  Every buffer the library
+ * allocates comes from its own stream-ordered pool on each device, which
+ * keeps up to 64 MiB of released blocks mapped so that plans can be built
+ * and destroyed cheaply.  This call synchronizes the current device and
+ * returns every released block of its pool to the device (blocks of live
+ * plans stay). */
+int merbit_release_cached_memory(void);
 
 /* ---------------- errors ---------------- */
 

@@ -79,6 +79,7 @@ SIGNATURES = {
     "merbit_plan_check": (C.c_int, [_P, _P]),
     "merbit_pagerank_step": (C.c_int, [_P, C.c_double, _P, _P, _P, _P, _P]),
     "merbit_plan_selftest_wait": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
+    "merbit_release_cached_memory": (C.c_int, []),
     "merbit_coo_sort": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int, _P]),
     "merbit_coo_to_csr": (C.c_int, [C.c_int32, _P, C.c_int32, _P, _P]),
     "merbit_outdegree_values": (C.c_int, [C.c_int32, C.c_int32, _P, _P, C.c_int, _P]),
@@ -160,6 +161,13 @@ def merge_coords(row_ptr: torch.Tensor, nnz: int, stride: int, count: int, strea
     _check(lib().merbit_merge_coords(_dptr(row_ptr), row_ptr.numel() - 1, nnz, stride, count,
                                      _dptr(cx), _dptr(cy), _stream_ptr(stream)))
     return cx, cy
+
+
+def release_cached_memory(device=None) -> None:
+    """Return the released blocks of the library's device memory pool
+    (merbit_release_cached_memory); blocks of live plans stay."""
+    with torch.cuda.device(device if device is not None else torch.cuda.current_device()):
+        _check(lib().merbit_release_cached_memory())
 
 
 def tile_dims(nrow: int, nnz: int, sigma: int) -> tuple[int, int]:

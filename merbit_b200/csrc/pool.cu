@@ -60,3 +60,16 @@ void dev_free(void* p, cudaStream_t s) {
 }
 
 }  // namespace merbit
+
+extern "C" int merbit_release_cached_memory(void) {
+    using namespace merbit;
+    int dev = 0;
+    MERBIT_CUDA(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (g_pools.find(dev) == g_pools.end()) return MERBIT_OK;  // nothing allocated yet
+    }
+    MERBIT_CUDA(cudaDeviceSynchronize());  // frees in flight reach the pool
+    MERBIT_CUDA(cudaMemPoolTrimTo(device_pool(dev), 0));
+    return MERBIT_OK;
+}
