@@ -1,8 +1,8 @@
 /* Measurement support for merbit_b200 (not part of the SpMV interface, and
  * with no counterpart in the reference).
  *
- * merbit_bench_gather: sum of x[idx[i]] over i < n (n a multiple of 16 is
- * covered fully), split over 2048 * SM-count threads that each keep 16
+ * merbit_bench_gather: sum of x[idx[i]] over i < n (n a multiple of 8 is
+ * covered fully), split over 2048 * SM-count threads that each keep 8
  * gathers in flight; out[t] receives thread t's sum.  Indices outside
  * [0, nx) read x[0]; idx must be 16-byte aligned and out must hold at least
  * 2048 * SM-count doubles.  Timing one launch gives the
