@@ -29,6 +29,9 @@ int fail(int status, const std::string& detail) {
 int cuda_fail(cudaError_t e, const char* where) {
     g_last_cuda = (int)e;
     g_detail = std::string(where) + ": " + cudaGetErrorString(e);
+    // un-latch a non-sticky error so that a later launch check of this
+    // thread does not report it again (a sticky error stays)
+    cudaGetLastError();
     return MERBIT_ERR_CUDA;
 }
 

@@ -47,6 +47,15 @@ cudaMemPool_t device_pool(int device) {
 
 int dev_alloc(void** p, size_t bytes, cudaStream_t s) {
     *p = nullptr;
+    // A stream-ordered allocation made while s is being captured would
+    // belong to the captured graph, not to the plan that keeps the pointer:
+    // refuse it, as cudaMalloc refuses allocation under capture.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    MERBIT_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(MERBIT_ERR_INVALID,
+                    "device allocation while the stream is being captured: make the first "
+                    "call of this kind (plan, SpMM slots, residual partials) before capture");
     int dev = 0;
     MERBIT_CUDA(cudaGetDevice(&dev));
     cudaMemPool_t pool = device_pool(dev);

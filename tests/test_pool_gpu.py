@@ -75,3 +75,29 @@ def test_reused_blocks_do_not_disturb_live_plans():
     assert b.check() is None and c.check() is None
     b.close()
     c.close()
+
+
+@pytest.mark.gpu
+def test_first_allocating_call_under_capture_is_refused():
+    """A call that must allocate (here the first SpMM at this k, which
+    allocates its carry slots) fails under stream capture instead of giving
+    the plan memory that the captured graph owns; outside capture it then
+    works."""
+    import torch
+
+    A = synth.zipf(20_000, 1.8, 5_000, 0.1, seed=50)
+    rp, col, v = to_cuda(A, "f64")
+    plan = mb.Plan(rp, col, v, ncol=A.ncol)
+    X = torch.from_numpy(synth.uniform(51, A.ncol * 4).reshape(A.ncol, 4)).cuda()
+    Y = torch.empty(A.nrow, 4, dtype=torch.float64, device="cuda")
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    with pytest.raises(mb.MerbitError) as ei:
+        with torch.cuda.graph(g, stream=s):
+            plan.spmm(X, Y, stream=s)
+    assert "captured" in ei.value.detail
+    del g
+    plan.spmm(X, Y)
+    torch.cuda.synchronize()
+    y_ref, yabs = O.spmm(A.row_ptr, A.col, A.vals, X.cpu().numpy(), k=4)
+    assert _rel_err(Y.cpu().numpy(), y_ref, yabs).max() <= 1e-12
