@@ -404,6 +404,10 @@ struct SpmvConfig {
     // gathers miss L1.
     int carveout;
     int cg;  // 1: x gathers cached in L2 only (ld.global.cg)
+    // Row-group kernel: 1 = a warp loads its row block's nonzeros as one
+    // contiguous run (coalesced) and stages the products in shared memory
+    // for the groups to reduce; 0 = each group reads its own row strided
+    int stg;
 };
 constexpr int kCarveoutL1 = 72;     // ~164 KB shared memory, the rest L1
 constexpr int kCarveoutL1Max = 58;  // ~132 KB shared memory

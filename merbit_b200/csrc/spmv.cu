@@ -274,7 +274,9 @@ constexpr SpmvConfig kCfgF64[] = {
     {3, 256, 4, 1, 0, 0},            {3, 256, 8, 1, 0, 0},
     {3, 256, 16, 1, 0, 0},           {3, 256, 32, 1, 0, 0},
     {3, 256, 8, 1, 0, 1},            {3, 256, 16, 1, 0, 1},
-    {3, 256, 2, 1, 0, 0}};
+    {3, 256, 2, 1, 0, 0},            {3, 256, 4, 1, 0, 0, 1},
+    {3, 256, 2, 1, 0, 0, 1},         {3, 256, 8, 1, 0, 0, 1},
+    {3, 256, 1, 1, 0, 0, 1}};
 constexpr SpmvConfig kCfgF32[] = {
     {1, 256, 15, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1, 1},
     {1, 256, 11, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1Max, 1},
@@ -286,7 +288,9 @@ constexpr SpmvConfig kCfgF32[] = {
     {3, 256, 4, 1, 0, 0},            {3, 256, 8, 1, 0, 0},
     {3, 256, 16, 1, 0, 0},           {3, 256, 32, 1, 0, 0},
     {3, 256, 8, 1, 0, 1},            {3, 256, 16, 1, 0, 1},
-    {3, 256, 2, 1, 0, 0}};
+    {3, 256, 2, 1, 0, 0},            {3, 256, 4, 1, 0, 0, 1},
+    {3, 256, 2, 1, 0, 0, 1},         {3, 256, 8, 1, 0, 0, 1},
+    {3, 256, 1, 1, 0, 0, 1}};
 
 template <int DT, int BLOCK, int IPT, bool VEC, bool RES>
 int launch_one_k(const SpmvLaunch& a, cudaStream_t s) {

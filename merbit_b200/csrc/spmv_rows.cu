@@ -59,7 +59,15 @@ __device__ __forceinline__ void finish_residual_only(LaunchState* st, double v, 
     }
 }
 
-template <int DT, int LPR, int WARPS, bool RES, bool CG>
+// STG (staged row blocks): the warp's RPW rows hold nonzeros [bs, be), one
+// contiguous run.  When it fits in CAP = 32 * UNR entries the warp loads it
+// coalesced (lane l takes bs + l, bs + l + 32, ...), gathers x, and stores the
+// products in its shared-memory slice; each group then sums its row from
+// there.  A lane sums the same nonzeros in the same order as without
+// staging (j, j + LPR, ... of its row).  Every col/vals line is touched once
+// per warp instead of once per unrolled step, which cuts the L1 wavefronts of
+// short rows several-fold.  Blocks that do not fit take the strided path.
+template <int DT, int LPR, int WARPS, bool RES, bool CG, bool STG = false>
 __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch a) {
     using Pr = Prec<DT>;
     using V = typename Pr::V;
@@ -81,11 +89,48 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch 
     const V* __restrict__ vals = static_cast<const V*>(a.vals);
     const X* __restrict__ xv = static_cast<const X*>(a.x);
     RowStore<Y, RES> out(a);
+    constexpr int CAP = 32 * UNR;
+    __shared__ P s_prod[STG ? WARPS : 1][STG ? CAP : 1];
+    P* __restrict__ sp = s_prod[STG ? (threadIdx.x >> 5) : 0];
     for (int r0 = gw * RPW; r0 < a.nrow; r0 += nw * RPW) {
         const int r = r0 + grp;
         Acc acc;
         acc.zero();
-        if (r < a.nrow) {
+        bool staged = false;
+        if (STG) {
+            int s = 0, e = 0;
+            if (r < a.nrow) {
+                s = __ldg(rp + r);
+                e = __ldg(rp + r + 1);
+            }
+            const int nb_rows = min(RPW, a.nrow - r0);  // >= 1: r0 < nrow
+            const int bs = __shfl_sync(0xFFFFFFFFu, s, 0);
+            const int be = __shfl_sync(0xFFFFFFFFu, e, (nb_rows - 1) * LPR);
+            if (be - bs <= CAP) {  // warp-uniform
+                int c[UNR];
+                V v[UNR];
+#pragma unroll
+                for (int u = 0; u < UNR; ++u) {
+                    const int k = bs + lane + 32 * u;
+                    c[u] = k < be ? __ldcs(col + k) : -1;
+                    v[u] = k < be ? __ldcs(vals + k) : V(0);
+                }
+                X xg[UNR];
+#pragma unroll
+                for (int u = 0; u < UNR; ++u)
+                    xg[u] = c[u] >= 0 ? (CG ? __ldcg(xv + c[u]) : __ldg(xv + c[u])) : (X)0;
+#pragma unroll
+                for (int u = 0; u < UNR; ++u)
+                    if (c[u] >= 0) sp[lane + 32 * u] = to_p(v[u]) * (P)xg[u];
+                __syncwarp();
+                // (clamped to the staged run, which a valid CSR never leaves)
+                const int i1 = min(e, be) - bs;
+                for (int i = max(s - bs, 0) + jl; i < i1; i += LPR) acc.add(sp[i]);
+                __syncwarp();  // the slice is rewritten by the next block
+                staged = true;
+            }
+        }
+        if (!staged && r < a.nrow) {
             const int s = __ldg(rp + r), e = __ldg(rp + r + 1);
             // steps of UNR * LPR nonzeros, predicated at the row end, so all
             // of a step's loads are in flight together
@@ -117,14 +162,14 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch 
                                     a.residual);
 }
 
-template <int DT, int LPR, bool RES, bool CG>
+template <int DT, int LPR, bool RES, bool CG, bool STG>
 int launch_rows_k(const SpmvLaunch& a, cudaStream_t s) {
     constexpr int WARPS = 8;
     static int grid_cap[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmv_rows: device ordinal >= 64");
-    auto kern = spmv_rows_kernel<DT, LPR, WARPS, RES, CG>;
+    auto kern = spmv_rows_kernel<DT, LPR, WARPS, RES, CG, STG>;
     if (grid_cap[dev] == 0) {
         int per_sm = 0, sms = 0;
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, 0);
@@ -141,15 +186,26 @@ int launch_rows_k(const SpmvLaunch& a, cudaStream_t s) {
     return e == cudaSuccess ? (int)MERBIT_OK : cuda_fail(e, "spmv_rows_kernel launch");
 }
 
-template <int DT, int LPR>
+template <int DT, int LPR, bool STG = false>
 int launch_rows_lpr(const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s) {
     if (a.residual)
-        return c.cg ? launch_rows_k<DT, LPR, true, true>(a, s) : launch_rows_k<DT, LPR, true, false>(a, s);
-    return c.cg ? launch_rows_k<DT, LPR, false, true>(a, s) : launch_rows_k<DT, LPR, false, false>(a, s);
+        return c.cg ? launch_rows_k<DT, LPR, true, true, STG>(a, s)
+                    : launch_rows_k<DT, LPR, true, false, STG>(a, s);
+    return c.cg ? launch_rows_k<DT, LPR, false, true, STG>(a, s)
+                : launch_rows_k<DT, LPR, false, false, STG>(a, s);
 }
 
 template <int DT>
 int launch_rows_dt(const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s) {
+    if (c.stg) {
+        switch (c.ipt) {  // lanes per row
+        case 1: return launch_rows_lpr<DT, 1, true>(c, a, s);
+        case 2: return launch_rows_lpr<DT, 2, true>(c, a, s);
+        case 4: return launch_rows_lpr<DT, 4, true>(c, a, s);
+        case 8: return launch_rows_lpr<DT, 8, true>(c, a, s);
+        }
+        return fail(MERBIT_ERR_INVALID, "spmv_rows: no such configuration");
+    }
     switch (c.ipt) {  // lanes per row
     case 2: return launch_rows_lpr<DT, 2>(c, a, s);
     case 4: return launch_rows_lpr<DT, 4>(c, a, s);
