@@ -34,6 +34,12 @@
  * events): each plan owns device scratch (carry slots, a launch counter)
  * that every launch reuses.  The reference is single-stream as well
  * (include/tile.cuh:596-603).
+ *
+ * Devices: a plan lives on the device that was current at
+ * merbit_plan_create, and its launches go to the calling thread's current
+ * device, which must be that one (streams belong to a device too).
+ * merbit_pagerank_step and merbit_plan_destroy switch to the plan's device
+ * for the call and restore the caller's current device.
  */
 #ifndef MERBIT_H
 #define MERBIT_H

@@ -417,9 +417,14 @@ int merbit_pagerank_step(merbit_plan plan, double damp, const void* d_x, const v
     if (!d_x || !d_y || !d_teleport) return fail(MERBIT_ERR_INVALID, "pagerank_step: null vector");
     if (d_x == d_y) return fail(MERBIT_ERR_INVALID, "pagerank_step: x and y must differ");
     if (!(damp >= 0.0 && damp <= 1.0)) return fail(MERBIT_ERR_INVALID, "pagerank_step: damp outside [0, 1]");
-    MERBIT_CUDA(cudaSetDevice(plan->device));
-    return run_spmv(plan, plan->cfg, damp, d_x, 1.0 - damp, d_y, (cudaStream_t)stream, d_teleport,
-                    d_residual);
+    // on the plan's device for this call; the caller's current device is restored
+    int cur = 0;
+    MERBIT_CUDA(cudaGetDevice(&cur));
+    if (cur != plan->device) MERBIT_CUDA(cudaSetDevice(plan->device));
+    const int st = run_spmv(plan, plan->cfg, damp, d_x, 1.0 - damp, d_y, (cudaStream_t)stream,
+                            d_teleport, d_residual);
+    if (cur != plan->device) cudaSetDevice(cur);
+    return st;
 }
 
 int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream) {

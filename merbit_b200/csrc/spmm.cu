@@ -618,7 +618,9 @@ int launch_spmm_cfg(const SpmmLaunch& a, cudaStream_t s) {
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmm: device ordinal >= 64");
     auto kern = spmm_kernel<DT, K, VW, ITEMS, WARPS, DV>;
-    if (grid_cap[dev] == 0) {
+    // per-device cache; threads that race here compute the same value
+    int cap = __atomic_load_n(&grid_cap[dev], __ATOMIC_ACQUIRE);
+    if (cap == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(spmm)");
@@ -626,10 +628,11 @@ int launch_spmm_cfg(const SpmmLaunch& a, cudaStream_t s) {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem);
         if (e != cudaSuccess) return cuda_fail(e, "occupancy(spmm)");
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        grid_cap[dev] = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
+        cap = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
+        __atomic_store_n(&grid_cap[dev], cap, __ATOMIC_RELEASE);
     }
     const long long need = ((long long)a.total_tiles + WARPS - 1) / WARPS;
-    const int grid = (int)(need < grid_cap[dev] ? need : grid_cap[dev]);
+    const int grid = (int)(need < cap ? need : cap);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3(WARPS * 32);

@@ -296,15 +296,17 @@ template <int DT, int BLOCK, int IPT, bool VEC, bool RES>
 int launch_one_k(const SpmvLaunch& a, cudaStream_t s) {
     using P = typename Prec<DT>::P;
     constexpr size_t smem = SpmvSmem<BLOCK, IPT, P>::bytes;
-    static bool attr_set[64] = {};  // per device ordinal
+    // per device ordinal; threads that race here set the same attribute
+    static int attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 64 && !attr_set[dev]) {
+    if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmv: device ordinal >= 64");
+    if (!__atomic_load_n(&attr_set[dev], __ATOMIC_ACQUIRE)) {
         cudaError_t e = cudaFuncSetAttribute(spmv_tile_kernel<DT, BLOCK, IPT, VEC, RES>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(spmv)");
-        attr_set[dev] = true;
+        __atomic_store_n(&attr_set[dev], 1, __ATOMIC_RELEASE);
     }
     spmv_tile_kernel<DT, BLOCK, IPT, VEC, RES><<<a.num_tiles, BLOCK, smem, s>>>(a);
     cudaError_t e = cudaGetLastError();

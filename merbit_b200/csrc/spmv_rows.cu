@@ -170,16 +170,19 @@ int launch_rows_k(const SpmvLaunch& a, cudaStream_t s) {
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmv_rows: device ordinal >= 64");
     auto kern = spmv_rows_kernel<DT, LPR, WARPS, RES, CG, STG>;
-    if (grid_cap[dev] == 0) {
+    // per-device cache; threads that race here compute the same value
+    int cap = __atomic_load_n(&grid_cap[dev], __ATOMIC_ACQUIRE);
+    if (cap == 0) {
         int per_sm = 0, sms = 0;
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, 0);
         if (e != cudaSuccess) return cuda_fail(e, "occupancy(spmv_rows)");
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        grid_cap[dev] = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
+        cap = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
+        __atomic_store_n(&grid_cap[dev], cap, __ATOMIC_RELEASE);
     }
     constexpr int RPB = WARPS * (32 / LPR);  // rows per block step
     const long long need = ((long long)a.nrow + RPB - 1) / RPB;
-    const int grid = (int)(need < grid_cap[dev] ? need : grid_cap[dev]);
+    const int grid = (int)(need < cap ? need : cap);
     if (RES && !a.partials) return fail(MERBIT_ERR_INVALID, "spmv_rows: residual without partials");
     kern<<<grid, WARPS * 32, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
