@@ -229,15 +229,19 @@ struct SpmmTile {
         V* s_val = reinterpret_cast<V*>(ws + rp_bytes + col_bytes);
         const V* vals = static_cast<const V*>(d.vals);
         const int nrp = d.nrow + 1;
-        auto bb = [](int s, int e, int n, int g, int esz) -> unsigned {
-            if (e <= s) return 0u;
+        // bulk copies need 16-byte aligned global addresses; an array whose
+        // base is not 16-byte aligned (a caller's offset view) is staged by
+        // plain loads instead (no transaction bytes)
+        auto bb = [](const void* src, int s, int e, int n, int g, int esz) -> unsigned {
+            if (e <= s || ((uintptr_t)src & 15u) != 0) return 0u;
             const int base = s & ~(g - 1), lim = n & ~(g - 1);
             const int b_end = min((e + g - 1) & ~(g - 1), lim);
             return b_end > base ? (unsigned)(b_end - base) * (unsigned)esz : 0u;
         };
-        const unsigned tot = bb(c0.y, c1.y + 1, nrp, 4, 4) + bb(c0.x, c1.x, d.nnz, 4, 4) +
-                             bb(c0.x, c1.x, d.nnz, GV, (int)sizeof(V)) +
-                             (DV ? bb(c0.x, c1.x, d.nnz, 4, 4) : 0u);
+        const unsigned tot = bb(d.row_ptr, c0.y, c1.y + 1, nrp, 4, 4) +
+                             bb(d.col, c0.x, c1.x, d.nnz, 4, 4) +
+                             bb(vals, c0.x, c1.x, d.nnz, GV, (int)sizeof(V)) +
+                             (DV ? bb(perm, c0.x, c1.x, d.nnz, 4, 4) : 0u);
         __syncwarp();
         if (lane == 0) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -249,6 +253,10 @@ struct SpmmTile {
             constexpr int GG = 16 / (int)sizeof(T);
             if (e <= s) return;
             const int base = s & ~(GG - 1), lim = n & ~(GG - 1);
+            if (((uintptr_t)src & 15u) != 0) {  // warp-uniform: plain loads
+                for (int i = s + lane; i < e; i += 32) dst[i - base] = src[i];
+                return;
+            }
             const int b_end = min((e + GG - 1) & ~(GG - 1), lim);
             if (b_end > base && lane == 0)
                 bulk_g2s(dst, src + base, (unsigned)(b_end - base) * (unsigned)sizeof(T), bar, pol);

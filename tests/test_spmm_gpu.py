@@ -116,3 +116,44 @@ def test_spmm_deterministic():
     ys = [plan.spmm(X).clone() for _ in range(10)]
     for y in ys[1:]:
         assert torch.equal(y.view(torch.int32), ys[0].view(torch.int32))
+
+
+def _offset(t: torch.Tensor) -> torch.Tensor:
+    """The same values at an address 4 (int32/f32) or 8 (f64) bytes past a
+    16-byte boundary, as a caller's slice of a larger buffer would be."""
+    buf = torch.empty(t.numel() + 1, dtype=t.dtype, device=t.device)
+    out = buf[1:]
+    out.copy_(t)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
+def test_spmm_and_batch_on_offset_arrays(dtype):
+    """row_ptr, col_idx and vals that do not start on a 16-byte boundary:
+    the SpMM stages them with plain loads instead of bulk copies (which need
+    16-byte aligned addresses), alone and inside a batch."""
+    mats = [synth.workload("zipf_small"),
+            csr_from_lengths([0, 3000, 0, 2, 9000, 1, 7, 0], ncol=12000, seed=4)]
+    plans, keep = [], []
+    for A in mats:
+        rp, col, v = to_cuda(A, dtype)
+        rp, col, v = _offset(rp), _offset(col), _offset(v)
+        keep.append((rp, col, v))
+        plans.append(mb.Plan(rp, col, v, ncol=A.ncol))
+        assert not plans[-1].info().vectorized
+    for k in (1, 3, 8):
+        for A, plan in zip(mats, plans):
+            X = _X(A.ncol, k, dtype)
+            Y = plan.spmm(torch.from_numpy(X).cuda())
+            torch.cuda.synchronize()
+            assert _check(A, dtype, Y.cpu().numpy(), X) <= TOL[dtype], (k, A.name)
+    Xh = [_X(A.ncol, 4, dtype, seed=20 + i) for i, A in enumerate(mats)]
+    Xs = [torch.from_numpy(X).cuda() for X in Xh]
+    Ys = [torch.full((A.nrow, 4), float("nan"), dtype=Xs[0].dtype, device="cuda") for A in mats]
+    b = mb.Batch(plans, Xs, Ys)
+    b.run()
+    torch.cuda.synchronize()
+    for A, X, Y in zip(mats, Xh, Ys):
+        assert _check(A, dtype, Y.cpu().numpy(), X) <= TOL[dtype], A.name
+    b.close()
