@@ -11,12 +11,15 @@ vector loads.  Each matrix runs through every configuration the tuner could
 pick, in every value type, and through the SpMM with a random k, against the
 extended-precision oracle with the tolerances of the other parity tests.
 """
+import math
+
 import numpy as np
 import pytest
 import torch
 
 import merbit_b200 as mb
 from merbit_b200 import synth
+from merbit_b200.autograd import SparseMatrix
 from oracle import oracle as O
 from tests.helpers import stored_values, to_cuda
 
@@ -25,10 +28,12 @@ XT = {"f64": np.float64, "f32": np.float32, "bf16": np.float32}
 SEEDS = range(16)
 
 
-def random_csr(seed: int) -> synth.CSR:
+def random_csr(seed: int, square: bool = False) -> synth.CSR:
     rng = np.random.default_rng(1000 + seed)
     nrow = int(rng.integers(1, 30_001))
     ncol = int(rng.integers(1, 60_001))
+    if square:
+        ncol = nrow
     u = rng.random(nrow)
     L = np.zeros(nrow, np.int64)  # u >= 0.85: empty
     short = u < 0.55
@@ -99,6 +104,119 @@ def test_random_csr_every_config_and_dtype(seed):
         assert (Ye.max() if Ye.size else 0.0) <= TOL[dtype], (dtype, k, float(Ye.max()))
         plan.check()
         plan.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", SEEDS)
+def test_random_partition_bit_exact(seed):
+    """merge_search coordinates and the reference TILE plan, bit for bit."""
+    A = random_csr(seed)
+    rp = torch.from_numpy(A.row_ptr).cuda()
+    total = A.nrow + A.nnz
+    for stride in (14, 448, 480, 3072):
+        count = min(total // stride + 2, 200_000)
+        cx, cy = mb.merge_coords(rp, A.nnz, stride, count)
+        ox, oy = O.merge_coords(A.row_ptr, stride, count)
+        assert np.array_equal(cx.cpu().numpy(), ox), stride
+        assert np.array_equal(cy.cpu().numpy(), oy), stride
+    for sigma in (14, 20):
+        tx, ty, desc = mb.tile_build(rp, A.nnz, sigma)
+        ox, oy, od = O.tile_plan(A.row_ptr, sigma)
+        assert np.array_equal(tx.cpu().numpy().view(np.uint32), ox)
+        assert np.array_equal(ty.cpu().numpy().view(np.uint32), oy)
+        d = desc.cpu().numpy()
+        assert np.array_equal(d.view(np.uint32) if sigma < 15 else d.view(np.uint64), od)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(8))
+def test_random_adjoints(seed):
+    """dX = A^T G through the transpose plan, dval = G[row].X[col], and the
+    fused backward, against the oracle (every fourth matrix on offset
+    arrays)."""
+    A = random_csr(seed)
+    rng = np.random.default_rng(seed)
+    k = int(rng.choice([1, 2, 4, 8, 16, 32]))
+    for dtype in ("f64", "f32"):
+        nt = XT[dtype]
+        X = synth.uniform(seed + 4, A.ncol * k).reshape(A.ncol, k).astype(nt)
+        G = synth.normal(seed + 6, A.nrow * k).reshape(A.nrow, k).astype(nt)
+        rp, col, v = to_cuda(A, dtype)
+        if seed % 4 == 3 and A.nnz > 0:
+            col, v = _offset(col), _offset(v)
+        M = SparseMatrix(rp, col, v, ncol=A.ncol)
+        Gd, Xd = torch.from_numpy(G).cuda(), torch.from_numpy(X).cuda()
+        vals = stored_values(A, dtype)
+        absv = np.abs(vals.astype(np.float64))
+        ref = O.spmm_t(A.row_ptr, A.col, vals, G, A.ncol)
+        den = O.spmm_t(A.row_ptr, A.col, absv, np.abs(G.astype(np.float64)), A.ncol)
+        refv = O.dval(A.row_ptr, A.col, G, X)
+        denv = O.dval(A.row_ptr, A.col, np.abs(G.astype(np.float64)), np.abs(X.astype(np.float64)))
+        tol = TOL[dtype]
+        dX = M.transpose_plan().spmm(Gd).cpu().numpy()
+        assert (np.abs(dX - ref) / np.maximum(den, 1e-300)).max(initial=0.0) <= tol, (dtype, k)
+        dv = M.dval(Gd, Xd).cpu().numpy()
+        assert (np.abs(dv - refv) / np.maximum(denv, 1e-300)).max(initial=0.0) <= tol, (dtype, k)
+        out = M.backward_fused(Gd, Xd)
+        if out is not None:
+            fX, fv = (t.cpu().numpy() for t in out)
+            assert (np.abs(fX - ref) / np.maximum(den, 1e-300)).max(initial=0.0) <= tol
+            assert (np.abs(fv - refv) / np.maximum(denv, 1e-300)).max(initial=0.0) <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(4))
+def test_random_batch(seed):
+    """Five random matrices in one persistent batched launch (random k and
+    value type, one of them on offset arrays), tuned, against the oracle."""
+    rng = np.random.default_rng(50 + seed)
+    k = int(rng.choice([1, 2, 4, 8, 16, 32]))
+    dtype = ("f64", "f32", "bf16")[seed % 3]
+    mats = [random_csr(100 + 5 * seed + j) for j in range(5)]
+    plans, Xh, Xs, Ys = [], [], [], []
+    for j, A in enumerate(mats):
+        rp, col, v = to_cuda(A, dtype)
+        if j == 2 and A.nnz > 0:
+            rp, col, v = _offset(rp), _offset(col), _offset(v)
+        plans.append(mb.Plan(rp, col, v, ncol=A.ncol))
+        X = synth.uniform(200 + j, A.ncol * k).reshape(A.ncol, k).astype(XT[dtype])
+        Xh.append(X)
+        Xs.append(torch.from_numpy(X).cuda())
+        Ys.append(torch.full((A.nrow, k), float("nan"), dtype=Xs[-1].dtype, device="cuda"))
+    b = mb.Batch(plans, Xs, Ys)
+    b.tune()
+    b.run()
+    torch.cuda.synchronize()
+    for A, X, Y in zip(mats, Xh, Ys):
+        Yo, Ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), X, k=k)
+        e = np.abs(Y.cpu().numpy().astype(np.float64) - Yo) / np.maximum(Ya, 1e-300)
+        assert e.max(initial=0.0) <= TOL[dtype], (dtype, k, A.name)
+    b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(4))
+def test_random_pagerank_step(seed):
+    """The fused PageRank step (damped SpMV + teleport + L1 residual) on
+    random square matrices, every configuration."""
+    A = random_csr(seed, square=True)
+    dtype = ("f64", "f32", "bf16", "f64")[seed]
+    x = synth.uniform(seed + 1, A.ncol).astype(XT[dtype])
+    t = synth.uniform(seed + 2, A.nrow).astype(XT[dtype])
+    yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+    ref = 0.85 * yo + 0.15 * t.astype(np.float64)
+    den = 0.85 * ya + 0.15 * np.abs(t.astype(np.float64))
+    rp, col, v = to_cuda(A, dtype)
+    plan = mb.Plan(rp, col, v)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    for idx, kind, _, ipt in plan.configs():
+        plan.set_config(idx)
+        res = torch.zeros(1, dtype=torch.float64, device="cuda")
+        y = plan.pagerank_step(xd, td, 0.85, residual=res).cpu().numpy()
+        assert O.rel_error(y, ref, den)[0] <= TOL[dtype], (dtype, idx, kind, ipt)
+        want = math.fsum(np.abs(y.astype(np.float64) - x.astype(np.float64)))
+        assert abs(res.item() - want) <= 1e-12 * max(want, 1e-300), (dtype, idx)
+    plan.check()
 
 
 def test_random_csr_generator_is_seeded_and_valid():
