@@ -219,6 +219,40 @@ def test_random_pagerank_step(seed):
     plan.check()
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(4))
+def test_random_front_end_to_spmv(seed):
+    """The harness front end end to end, as Fun_Merbit runs it: shuffled COO
+    triplets (duplicates included) -> stable sort by row -> coo_to_csr ->
+    plan -> SpMV, against the oracle on the same matrix built by numpy; and
+    the loader's 1/outdegree weights against numpy."""
+    A = random_csr(200 + seed)
+    dtype = ("f64", "f32", "bf16", "f64")[seed]
+    rng = np.random.default_rng(300 + seed)
+    rows = np.repeat(np.arange(A.nrow, dtype=np.int32), np.diff(A.row_ptr))
+    perm = rng.permutation(A.nnz)
+    td = {"f64": torch.float64, "f32": torch.float32, "bf16": torch.bfloat16}[dtype]
+    dr = torch.from_numpy(rows[perm]).cuda()
+    # values stored as the oracle's stored_values rounds them
+    _, dc, dv = to_cuda(synth.CSR(A.row_ptr, A.col[perm], A.vals[perm], A.ncol, "shuffled"), dtype)
+    mb.coo_sort(dr, dc, dv)  # by (row, col), stable
+    order = np.lexsort((A.col[perm], rows[perm]))
+    assert np.array_equal(dr.cpu().numpy(), rows[perm][order])
+    assert np.array_equal(dc.cpu().numpy(), A.col[perm][order])
+    rp = mb.coo_to_csr(dr, A.nrow)
+    assert np.array_equal(rp.cpu().numpy(), A.row_ptr)
+    B = synth.CSR(A.row_ptr, A.col[perm][order], A.vals[perm][order], A.ncol, "sorted")
+    x = synth.uniform(seed + 9, A.ncol).astype(XT[dtype])
+    yo, ya = O.spmm(B.row_ptr, B.col, stored_values(B, dtype), x)
+    plan = mb.Plan(rp, dc, dv, ncol=A.ncol)
+    plan.tune(torch.from_numpy(x).cuda())
+    y = plan.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert O.rel_error(y, yo, ya)[0] <= TOL[dtype]
+    w = mb.outdegree_values(dr, A.nrow, td).to(torch.float64).cpu().numpy()
+    ref = torch.from_numpy(1.0 / np.diff(A.row_ptr)[rows]).to(td).to(torch.float64).numpy()
+    assert np.array_equal(w, ref)
+
+
 def test_random_csr_generator_is_seeded_and_valid():
     """CPU: the generator is deterministic and yields a valid CSR with the
     mixture the GPU test relies on."""
