@@ -261,3 +261,42 @@ def test_row_groups_edge_cases(name, A, dtype):
         assert O.rel_error(y, yo, ya)[0] <= TOL[dtype], (idx, lpr)
         assert np.all(y[np.diff(A.row_ptr) == 0] == 0)
     plan.check()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("workload", ["zipf_small", "stencil27_small"])
+def test_graph_replay_every_config(dtype, workload):
+    """Every configuration captured in a CUDA graph and replayed: three SpMVs
+    per graph (an odd count, so the launch epoch's parity differs from one
+    replay to the next), four replays with new x each time, no host-side
+    reset in between; every y against the oracle."""
+    A = synth.workload(workload)
+    rp, col, v = to_cuda(A, dtype)
+    plan = mb.Plan(rp, col, v, ncol=A.ncol)
+    nt = np.float64 if dtype == "f64" else np.float32
+    xs = [torch.from_numpy(_x(A, dtype, seed=40 + j)).cuda() for j in range(3)]
+    ys = [torch.empty(A.nrow, dtype=xs[0].dtype, device="cuda") for _ in range(3)]
+    s = torch.cuda.Stream()
+    for idx, kind, _, _ in plan.configs():
+        plan.set_config(idx)
+        plan.spmv(xs[0], ys[0])  # first launch outside capture (function attributes)
+        torch.cuda.synchronize()
+        s.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            for j in range(3):
+                plan.spmv(xs[j], ys[j], stream=s)
+        for rep in range(4):
+            xh = [synth.uniform(100 * rep + 10 * idx + j, A.ncol).astype(nt) for j in range(3)]
+            for j in range(3):
+                xs[j].copy_(torch.from_numpy(xh[j]))
+                ys[j].fill_(float("nan"))
+            g.replay()
+            torch.cuda.synchronize()
+            for j in range(3):
+                yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), xh[j])
+                e = O.rel_error(ys[j].cpu().numpy(), yo, ya)[0]
+                assert e <= TOL[dtype], (idx, kind, rep, j, e)
+        del g
+        plan.check()
