@@ -68,6 +68,9 @@ def parse_args():
     ap.add_argument("--k", type=int, default=8,
                     help="right-hand sides of the batched form (--workload rmat_batch128)")
     ap.add_argument("--batch", type=int, default=128, help="matrices of the batched form")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the secondary forms (stencil precision form, batched form, "
+                         "differentiation form) that the default power-law run adds")
     return ap.parse_args()
 
 
@@ -210,8 +213,25 @@ def load(args):
     from merbit_b200 import synth
 
     A = synth.workload(args.workload)
-    x = synth.uniform(1, A.ncol)
+    x = synth.workload_x(args.workload, A.ncol)
     return A, x
+
+
+L2_BYTES = 126 * 1024 * 1024
+
+
+def l2_note(A, dtype: str) -> str:
+    if alg_bytes(A, dtype) > L2_BYTES:
+        return ("inputs larger than L2 (the matrix is streamed from HBM every step); "
+                "value_l2_flushed flushes L2 before every launch")
+    return ("matrix fits in L2 (L2-resident between back-to-back steps); "
+            "value_l2_flushed flushes L2 before every launch")
+
+
+def workload_config(args, A) -> dict:
+    """The workload both arms print, as one identical dict."""
+    return {"workload": args.workload, "nrow": A.nrow, "ncol": A.ncol, "nnz": A.nnz,
+            "values": args.dtype, "k": 1, "l2": l2_note(A, args.dtype)}
 
 
 def cpu_baseline(A, x, seconds: float):
@@ -278,6 +298,347 @@ def traffic_from_profile(workload: str, dtype: str):
         with open(p) as f:
             return json.load(f).get("dram_bytes_per_launch")
     return None
+
+
+def fast_tiles(rp, A, info) -> dict:
+    """Tiles that end no row -- the single-row path (the reference's
+    fast_track, include/tile.cuh:267-290; counted by its tile_desc_kernel,
+    include/tile.cuh:178-210).  For the reference plan format (32 lanes x 14
+    items, the fast flag in tile_y's MSB) and for the partition of the
+    kernel in use (its nr == 0 tiles), the fraction of tiles and of
+    nonzeros on that path."""
+    import torch
+
+    import merbit_b200 as mb
+
+    out = {}
+    tx, ty, _ = mb.tile_build(rp, A.nnz, 14)
+    t = ty.numel() - 1
+    fast = (ty[:-1].view(torch.int32) < 0)  # MSB set
+    nz = (tx[1:] - tx[:-1]).to(torch.int64)
+    out["reference_plan_sigma14"] = {
+        "tiles": int(t), "fast_tiles": int(fast.sum()),
+        "frac_tiles": round(float(fast.sum()) / max(t, 1), 4),
+        "frac_nnz": round(float(nz[fast].sum()) / max(A.nnz, 1), 4)}
+    if info.kind in (0, 1) and info.num_tiles > 0:
+        T = info.num_tiles
+        cx, cy = mb.merge_coords(rp, A.nnz, info.tile_items, T + 1)
+        f = cy[1:] == cy[:-1]
+        n = (cx[1:] - cx[:-1]).to(torch.int64)
+        out["kernel_partition"] = {
+            "tile_items": info.tile_items, "tiles": int(T), "single_row_tiles": int(f.sum()),
+            "frac_tiles": round(float(f.sum()) / T, 4),
+            "frac_nnz": round(float(n[f].sum()) / max(A.nnz, 1), 4)}
+    else:
+        out["kernel_partition"] = None  # row-group kernel: no merge-path tiles
+    return out
+
+
+def graph_time(launch, steps: int, dev, stream, local: int = 0):
+    """Mean device time (ms) of one launch(stream) call: `steps` calls are
+    captured into one CUDA graph, replayed once untimed (upload) and once
+    inside CUDA events; NVML clocks are sampled meanwhile."""
+    import torch
+
+    g = torch.cuda.CUDAGraph()
+    cap = torch.cuda.Stream(dev)
+    cap.wait_stream(stream)
+    with torch.cuda.graph(g, stream=cap):
+        for _ in range(steps):
+            launch(cap)
+    stream.wait_stream(cap)
+    g.replay()
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(local).start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.replay()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    sampler.stop()
+    del g
+    return e0.elapsed_time(e1) / steps, sampler.summary()
+
+
+def component_error(y, y_ref, y_abs) -> dict:
+    """max and median of |y - y_ref| / max(sum_j |a_ij x_j|, tiny)."""
+    e = np.abs(np.asarray(y, np.float64) - y_ref) / np.maximum(y_abs, 1e-300)
+    if e.size == 0:
+        return {"max": 0.0, "median": 0.0}
+    return {"max": float(e.max()), "median": float(np.median(e))}
+
+
+def spmv_form(A, dtype: str, rp, col, vals64, x64, steps: int, dev, stream, peak: float,
+              workload: str) -> dict:
+    """One tuned SpMV of A with values stored as `dtype` (x FP64 for FP64
+    values, FP32 otherwise), timed over `steps` graph-captured launches, with
+    its error against an FP64 SpMV (the OpenMP oracle) of the inputs as
+    stored."""
+    import torch
+
+    import merbit_b200 as mb
+    from oracle import oracle as O
+
+    vt = {"f64": torch.float64, "f32": torch.float32, "bf16": torch.bfloat16}[dtype]
+    xt = torch.float64 if dtype == "f64" else torch.float32
+    vals = vals64.to(vt)
+    x = x64.to(xt)
+    y = torch.empty(A.nrow, dtype=xt, device=dev)
+    plan = mb.Plan(rp, col, vals, ncol=A.ncol)
+    plan.tune(x)
+    info = plan.info()
+    for _ in range(3):
+        plan.spmv(x, y)
+    ms, clk = graph_time(lambda s: plan.spmv(x, y, stream=s), steps, dev, stream)
+    plan.check()
+    B = alg_bytes(A, dtype)
+    gbs = B / (ms * 1e-3) / 1e9
+    vs = vals.to(torch.float64).cpu().numpy()
+    xs = x.to(torch.float64).cpu().numpy()
+    ys, _ = O.spmv_omp_f64(A.row_ptr, A.col, vs, xs)
+    ya = O.spmv_abs_omp_f64(A.row_ptr, A.col, vs, xs)
+    out = {
+        "ms": round(ms, 5), "gbs": round(gbs, 2), "gflops": round(2.0 * A.nnz / (ms * 1e-3) / 1e9, 2),
+        "algorithmic_bytes": B,
+        "roofline": {"bound": "hbm", "achieved": round(gbs, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(gbs / peak, 4),
+                     "traffic": traffic_from_profile(workload, dtype),
+                     "kernel": KERNEL_OF_KIND[info.kind]},
+        "kernel": f"{KERNEL_OF_KIND[info.kind]} block={info.block} ipt={info.items_per_thread} "
+                  f"tile_items={info.tile_items} l1_carveout={info.l1_carveout} "
+                  f"gather_l2_only={int(info.gather_l2_only)}",
+        "err_vs_fp64_stored_inputs": component_error(y.cpu().numpy(), ys, ya),
+        "clocks": clk,
+    }
+    plan.close()
+    return out
+
+
+def batch_forms(steps: int, dev, stream, peak: float, count: int = 128, ks=(1, 32)) -> dict:
+    """The batched form against the plain form on the same matrices at the
+    same k: `count` R-MAT matrices (seed 2) with FP32 values in one
+    persistent, graph-captured, tuned launch, against one plain FP64 launch
+    per matrix (tuned SpMV at k = 1, SpMM otherwise), also graph-captured."""
+    import torch
+
+    import merbit_b200 as mb
+    from merbit_b200 import synth
+
+    t0 = time.perf_counter()
+    specs = synth.batch_rmat_specs(count, seed=2)
+    mats = [synth.rmat(n, d, seed=sd) for n, d, sd in specs]
+    t_gen = time.perf_counter() - t0
+    nnz = sum(A.nnz for A in mats)
+    dev_mats = []
+    for A in mats:
+        rp = torch.from_numpy(A.row_ptr).to(dev)
+        col = torch.from_numpy(np.ascontiguousarray(A.col)).to(dev)
+        v64 = torch.from_numpy(np.ascontiguousarray(A.vals)).to(dev)
+        dev_mats.append((rp, col, v64))
+    out = {"matrices": count, "nnz": nnz, "rows": sum(A.nrow for A in mats),
+           "generate_s": round(t_gen, 2)}
+    for k in ks:
+        Xh = [synth.uniform(100 + i, A.ncol * k).astype(np.float32).reshape(A.ncol, k)
+              for i, A in enumerate(mats)]
+        # batched form: FP32 values, one launch
+        p32, X32, Y32 = [], [], []
+        for (rp, col, v64), A, X in zip(dev_mats, mats, Xh):
+            p32.append(mb.Plan(rp, col, v64.to(torch.float32), ncol=A.ncol))
+            X32.append(torch.from_numpy(X).to(dev))
+            Y32.append(torch.empty(A.nrow, k, dtype=torch.float32, device=dev))
+        batch = mb.Batch(p32, X32, Y32)
+        batch.tune()
+        binfo = batch.info()
+        batch.run()
+        ms_b, clk_b = graph_time(lambda s: batch.run(stream=s), steps, dev, stream)
+        # plain form: FP64 values, x and accumulation, one launch per matrix
+        p64, X64, Y64 = [], [], []
+        for (rp, col, v64), A, X in zip(dev_mats, mats, X32):
+            p = mb.Plan(rp, col, v64, ncol=A.ncol)
+            x64 = X.to(torch.float64)
+            if k == 1:
+                x64 = x64[:, 0].contiguous()
+                p.tune(x64)
+                Y64.append(torch.empty(A.nrow, dtype=torch.float64, device=dev))
+            else:
+                Y64.append(torch.empty(A.nrow, k, dtype=torch.float64, device=dev))
+            p64.append(p)
+            X64.append(x64)
+
+        def plain(s):
+            for p, x, y in zip(p64, X64, Y64):
+                if k == 1:
+                    p.spmv(x, y, stream=s)
+                else:
+                    p.spmm(x, y, stream=s)
+
+        plain(stream)
+        ms_p, clk_p = graph_time(plain, steps, dev, stream)
+        # error of the batched FP32 result against the plain FP64 one, whose
+        # denominators sum |a x| come from the same FP64 kernels on |A|, |X|
+        torch.cuda.synchronize(dev)
+        worst, meds = 0.0, []
+        for (rp, col, v64), A, p, x, y64, y32 in zip(dev_mats, mats, p64, X64, Y64, Y32):
+            pa = mb.Plan(rp, col, v64.abs(), ncol=A.ncol)
+            ya = pa.spmv(x.abs()) if k == 1 else pa.spmm(x.abs())
+            e = ((y32.reshape(y64.shape).double() - y64).abs() /
+                 ya.clamp_min(1e-300)).flatten()
+            if e.numel():
+                worst = max(worst, float(e.max()))
+                meds.append(float(e.median()))
+            pa.close()
+        b64 = sum(alg_bytes(A, "f64", k) for A in mats)
+        b32 = binfo["algorithmic_bytes"]
+        out[f"k{k}"] = {
+            "batched_f32": {
+                "ms": round(ms_b, 4), "gflops": round(2.0 * nnz * k / (ms_b * 1e-3) / 1e9, 2),
+                "gbs": round(b32 / (ms_b * 1e-3) / 1e9, 2),
+                "roofline": {"bound": "hbm", "achieved": round(b32 / (ms_b * 1e-3) / 1e9, 2),
+                             "peak": peak, "unit": "GB/s",
+                             "frac": round(b32 / (ms_b * 1e-3) / 1e9 / peak, 4),
+                             "traffic": batch_traffic(k)},
+                "launches_per_step": 1, "tile_items": binfo["tile_items"],
+                "vector_width": binfo["vector_width"], "clocks": clk_b,
+                "err_vs_plain_fp64": {"max": worst, "median": float(np.median(meds))},
+            },
+            "plain_f64": {
+                "ms": round(ms_p, 4), "gflops": round(2.0 * nnz * k / (ms_p * 1e-3) / 1e9, 2),
+                "gbs": round(b64 / (ms_p * 1e-3) / 1e9, 2), "launches_per_step": count,
+                "clocks": clk_p,
+                "kernel": "tuned SpMV per matrix" if k == 1 else "merge-path SpMM per matrix",
+            },
+        }
+        batch.close()
+        for p in p32 + p64:
+            p.close()
+        del X32, Y32, X64, Y64, Xh
+    return out
+
+
+def batch_traffic(k: int):
+    p = os.path.join(ROOT, "profiles", f"spmm_f32_rmat128_k{k}_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+def diff_measure(A, k: int, steps: int, dev, stream) -> dict:
+    """Differentiation form: forward Y = A X and forward + backward (dX =
+    A^T G and dval from one fused launch where the operands allow), FP32
+    values, k right-hand sides; mean ms over `steps` back-to-back steps."""
+    import torch
+
+    from merbit_b200 import synth
+    from merbit_b200.autograd import SparseMatrix
+
+    rp = torch.from_numpy(A.row_ptr).to(dev)
+    col = torch.from_numpy(A.col).to(dev)
+    vals = torch.from_numpy(A.vals.astype(np.float32)).to(dev)
+    M = SparseMatrix(rp, col, vals, ncol=A.ncol)
+    X = torch.from_numpy(synth.workload_x("zipf_1m_diff", A.ncol, k).astype(np.float32)).to(dev)
+    G = torch.from_numpy(synth.normal(3, A.nrow * k).astype(np.float32).reshape(A.nrow, k)).to(dev)
+    T = M.transpose_plan()
+    Y = torch.empty(A.nrow, k, dtype=torch.float32, device=dev)
+    dX = torch.empty(A.ncol, k, dtype=torch.float32, device=dev)
+
+    def fwd():
+        M.plan.spmm(X, Y)
+
+    fused = M.backward_fused(G, X) is not None
+
+    def bwd():
+        if not fused or M.backward_fused(G, X) is None:
+            T.spmm(G, dX)
+            M.dval(G, X)
+
+    for _ in range(3):
+        fwd()
+        bwd()
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(0).start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fwd()
+    e1.record(stream)
+    for _ in range(steps):
+        fwd()
+        bwd()
+    e2.record(stream)
+    torch.cuda.synchronize(dev)
+    sampler.stop()
+    M.plan.check()
+    t_f = e0.elapsed_time(e1) / steps
+    t_fb = e1.elapsed_time(e2) / steps
+    return {"fwd_ms": round(t_f, 4), "fwd_bwd_ms": round(t_fb, 4),
+            "fwd_bwd_over_fwd": round(t_fb / t_f, 3),
+            "backward": "fused transpose SpMM + dval (merbit_spmm_dval)" if fused
+                        else "transpose SpMM, then dval",
+            "launches_per_step": 2 if fused else 3, "fused": fused, "clocks": sampler.summary()}
+
+
+def secondary_forms(args, A_zipf, rp, col, vals64, x64, dev, stream, peak,
+                    ms_headline: float) -> tuple[dict, dict]:
+    """The precision, batched and differentiation forms of the default run,
+    each on its own benchmark matrix, plus the like-for-like ratios of the
+    mixed or batched forms over the plain FP64 form."""
+    import torch
+
+    from merbit_b200 import synth
+
+    steps = args.steps
+    forms, ratios = {}, {}
+    t0 = time.perf_counter()
+    # precision form on the power-law matrix itself (same matrix, same k = 1)
+    zf = {d: spmv_form(A_zipf, d, rp, col, vals64, x64, steps, dev, stream, peak, "zipf_2m")
+          for d in ("f32", "bf16")}
+    forms["zipf_2m"] = zf
+    # 27-point stencil 160^3 in FP64, FP32 and BF16
+    S = synth.workload("stencil27_160")
+    srp = torch.from_numpy(S.row_ptr).to(dev)
+    scol = torch.from_numpy(S.col).to(dev)
+    sv = torch.from_numpy(S.vals).to(dev)
+    sx = torch.from_numpy(synth.workload_x("stencil27_160", S.ncol)).to(dev)
+    st = {d: spmv_form(S, d, srp, scol, sv, sx, steps, dev, stream, peak, "stencil27_160")
+          for d in ("f64", "f32", "bf16")}
+    forms["stencil27_160"] = {"nrow": S.nrow, "nnz": S.nnz, **st}
+    del srp, scol, sv, sx, S
+    torch.cuda.empty_cache()
+    # batched form, k = 1 and 32
+    bf = batch_forms(steps, dev, stream, peak)
+    forms["rmat_batch128"] = bf
+    torch.cuda.empty_cache()
+    # differentiation form: Zipf(1.8) 1M rows, k = 16
+    D = synth.workload("zipf_1m_diff")
+    forms["zipf_1m_diff_k16"] = {"nrow": D.nrow, "nnz": D.nnz,
+                                 **diff_measure(D, 16, steps, dev, stream)}
+    del D
+    torch.cuda.empty_cache()
+    forms["wall_s"] = round(time.perf_counter() - t0, 1)
+
+    def ratio(plain_ms, mixed_ms, err, what):
+        return {"speedup": round(plain_ms / mixed_ms, 3), "plain_f64_ms": plain_ms,
+                "mixed_ms": mixed_ms, "err_max": err["max"], "err_median": err["median"],
+                "within_1e-6": bool(err["max"] <= 1e-6), "compares": what}
+
+    for d in ("f32", "bf16"):
+        ratios[f"zipf_2m_{d}_vs_f64"] = ratio(
+            ms_headline, zf[d]["ms"], zf[d]["err_vs_fp64_stored_inputs"],
+            f"power-law 2M, k = 1: {d} values + f32 x vs plain FP64, same matrix")
+        ratios[f"stencil27_160_{d}_vs_f64"] = ratio(
+            st["f64"]["ms"], st[d]["ms"], st[d]["err_vs_fp64_stored_inputs"],
+            f"27-point stencil 160^3, k = 1: {d} values + f32 x vs plain FP64, same matrix")
+    for k in (1, 32):
+        b = bf[f"k{k}"]
+        ratios[f"rmat_batch128_k{k}_batched_f32_vs_f64"] = ratio(
+            b["plain_f64"]["ms"], b["batched_f32"]["ms"], b["batched_f32"]["err_vs_plain_fp64"],
+            f"128 R-MAT matrices, k = {k}: one batched FP32 launch vs one plain FP64 launch "
+            "per matrix, same matrices and right-hand sides")
+    return forms, ratios
 
 
 def run_ours(args):
@@ -459,20 +820,15 @@ def run_ours(args):
         "dtype": args.dtype,
         "data": "synthetic (seeded generator merbit_b200/synth.py; the reference's "
                 "Matrix Market graphs are not available)",
-        "config": {
-            "workload": args.workload,
-            "nrow": A.nrow, "ncol": A.ncol, "nnz": A.nnz,
-            "values": args.dtype, "k": 1,
-            "l2": "inputs larger than L2 (matrix streamed from HBM every step); "
-                  "value_l2_flushed flushes L2 before every launch",
-            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-            "launch": "the K timed SpMV launches captured in one CUDA graph, replayed once",
-            "kernel": f"{KERNEL_OF_KIND[info.kind]} "
-                      f"block={info.block} ipt={info.items_per_thread} "
-                      f"tile_items={info.tile_items} tiles={info.num_tiles} "
-                      f"vectorized={int(info.vectorized)} l1_carveout={info.l1_carveout} "
-                      f"gather_l2_only={int(info.gather_l2_only)}",
-        },
+        "config": workload_config(args, A),
+        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+        "launch": "the K timed SpMV launches captured in one CUDA graph, replayed once",
+        "kernel": f"{KERNEL_OF_KIND[info.kind]} "
+                  f"block={info.block} ipt={info.items_per_thread} "
+                  f"tile_items={info.tile_items} tiles={info.num_tiles} "
+                  f"vectorized={int(info.vectorized)} l1_carveout={info.l1_carveout} "
+                  f"gather_l2_only={int(info.gather_l2_only)}",
+        "fast_tiles": fast_tiles(rp, A, info),
         "pct_hbm_peak": round(100.0 * achieved / peak, 2),
         "gflops": round(ws * 2.0 * A.nnz / (ms * 1e-3) / 1e9, 2),
         "value_l2_flushed": round(ws * B / (ms_cold * 1e-3) / 1e9, 2),
@@ -513,6 +869,10 @@ def run_ours(args):
         },
         "clocks": sampler.summary(),
     }
+    if ws == 1 and not args.no_forms and args.workload == "zipf_2m" and args.dtype == "f64":
+        forms, ratios = secondary_forms(args, A, rp, col, vals, xd, dev, stream, peak, ms)
+        out["forms"] = forms
+        out["mixed_vs_plain"] = ratios
     if ws == 1 and not args.no_cpu_baseline:
         y_cpu, t_cpu, threads, reps = cpu_baseline(A, x, args.cpu_seconds)
         out["cpu_baseline"] = {
@@ -702,57 +1062,16 @@ def run_diff(args):
     import torch
 
     from merbit_b200 import synth
-    from merbit_b200.autograd import SparseMatrix
 
     ws, rank, local = dist_setup(args)
     dev = torch.device("cuda", local)
     A = synth.workload(args.workload)
     k = args.k
-    rp = torch.from_numpy(A.row_ptr).to(dev)
-    col = torch.from_numpy(A.col).to(dev)
-    vals = torch.from_numpy(A.vals.astype(np.float32)).to(dev)
-    M = SparseMatrix(rp, col, vals, ncol=A.ncol)
-    X = torch.from_numpy(synth.uniform(3, A.ncol * k).astype(np.float32).reshape(A.ncol, k)).to(dev)
-    G = torch.from_numpy(synth.normal(3, A.nrow * k).astype(np.float32).reshape(A.nrow, k)).to(dev)
-    T = M.transpose_plan()
-    Y = torch.empty(A.nrow, k, dtype=torch.float32, device=dev)
-    dX = torch.empty(A.ncol, k, dtype=torch.float32, device=dev)
-
-    def fwd():
-        M.plan.spmm(X, Y)
-
-    fused = M.backward_fused(G, X) is not None
-
-    def bwd():
-        # one launch (dX and dval together) where the shape allows it
-        if not fused or M.backward_fused(G, X) is None:
-            T.spmm(G, dX)
-            M.dval(G, X)
-
-    for _ in range(max(args.warmup, 3)):
-        fwd()
-        bwd()
-    torch.cuda.synchronize(dev)
-    cur = torch.cuda.current_stream(dev)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e2 = torch.cuda.Event(enable_timing=True)
-    n = args.steps
-    sampler = ClockSampler(local).start()
     barrier(ws)
-    e0.record(cur)
-    for _ in range(n):
-        fwd()
-    e1.record(cur)
-    for _ in range(n):
-        fwd()
-        bwd()
-    e2.record(cur)
-    torch.cuda.synchronize(dev)
+    d = diff_measure(A, k, args.steps, dev, torch.cuda.current_stream(dev))
     barrier(ws)
-    sampler.stop()
-    t_f = allreduce_max(ws, e0.elapsed_time(e1) / n)
-    t_fb = allreduce_max(ws, e1.elapsed_time(e2) / n)
+    t_f = allreduce_max(ws, d["fwd_ms"])
+    t_fb = allreduce_max(ws, d["fwd_bwd_ms"])
     if rank != 0:
         if ws > 1:
             import torch.distributed as dist
@@ -765,24 +1084,23 @@ def run_diff(args):
         "metric": METRIC,
         "value": round(ws * B / (t_f * 1e-3) / 1e9, 2),
         "unit": "GB/s",
-        "n_gpus": ws, "steps": n, "warmup": max(args.warmup, 3),
+        "n_gpus": ws, "steps": args.steps, "warmup": max(args.warmup, 3),
         "ms_per_step": round(t_f, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded Zipf(1.8) generator, merbit_b200/synth.py)",
-        "config": {"workload": args.workload, "nrow": A.nrow, "nnz": A.nnz, "k": k,
-                   "values": "f32"},
+        "config": {"workload": args.workload, "nrow": A.nrow, "ncol": A.ncol, "nnz": A.nnz,
+                   "values": "f32", "k": k, "l2": "inputs larger than L2"},
         "fwd_ms": round(t_f, 4),
         "fwd_bwd_ms": round(t_fb, 4),
         "fwd_bwd_over_fwd": round(t_fb / t_f, 3),
-        "gpu_launches": (3 if fused else 4) * n,
-        "backward": "fused transpose SpMM + dval (merbit_spmm_dval)" if fused
-                    else "transpose SpMM, then dval",
+        "gpu_launches": (1 + d["launches_per_step"]) * args.steps,
+        "backward": d["backward"],
         "roofline": {"bound": "hbm", "achieved": round(B / (t_f * 1e-3) / 1e9, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(B / (t_f * 1e-3) / 1e9 / peak, 4),
                      "peak_source": f"{peak_src} hbm_gbs", "traffic": None,
                      "kernel": "spmm_kernel (forward)"},
-        "clocks": sampler.summary(),
+        "clocks": d["clocks"],
     }
     print(json.dumps(out), flush=True)
 
@@ -833,8 +1151,7 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded generator merbit_b200/synth.py)",
-        "config": {"workload": args.workload, "nrow": A.nrow, "ncol": A.ncol, "nnz": A.nnz,
-                   "values": "f64", "k": 1},
+        "config": workload_config(args, A),
         "cpu_baseline": {
             "value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
             "sample": f"full {args.workload} matrix per step, median of {len(per_step)} steps; "

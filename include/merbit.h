@@ -25,7 +25,7 @@
  *   merbit_plan_transpose + merbit_spmm, merbit_dval, merbit_spmm_dval
  *                         adjoints dX = A^T G and dval = G[row].X[col]
  *   merbit_plan_tune, merbit_plan_set_config   the configuration table
- *   merbit_spmv_noalloc   one SpMV that allocates nothing
+ *   merbit_spmv_noalloc   one SpMV that allocates nothing (+ _check, _selftest_wait)
  *   merbit_plan_check, merbit_plan_selftest_wait   device-side failure status
  *   merbit_release_cached_memory   empties the library's device memory pool
  *
@@ -89,6 +89,7 @@ typedef struct merbit_plan_info {
     int32_t gather_l2_only;  /* 1: x gathers bypass L1 allocation (ld.global.cg) */
     int64_t metadata_bytes;  /* partition + carry scratch held by the plan */
     double algorithmic_bytes;/* compulsory bytes of one SpMV, y = A x */
+    int32_t max_row_len;     /* longest row (nonzeros); part of the tuning signature */
 } merbit_plan_info;
 
 /* ---------------- reference-format partition (parity surface) ---------------- */
@@ -227,11 +228,14 @@ typedef struct merbit_batch_s* merbit_batch;
 
 typedef struct merbit_batch_info {
     int32_t count, k, dtype;
-    int32_t tile_items;    /* merge items per warp tile */
+    int32_t tile_items;    /* merge items per warp tile (kernel 0; per matrix for kernel 1) */
     int32_t vector_width;  /* RHS values per lane */
     int32_t total_tiles;
     int64_t nnz;
     double algorithmic_bytes; /* sum over matrices of one SpMM's compulsory bytes */
+    int32_t kernel;        /* 0: SpMM kernel (lane groups); 1: warp-tile kernel (k = 1) */
+    int32_t variant;       /* kernel 1: 0 L1 gathers, all shared memory; 1 L1 gathers with a
+                              72% shared-memory carveout; 2 L2-only gathers, 72% carveout */
 } merbit_batch_info;
 
 /* A batch of `count` plans (same dtype) multiplied by k in {1,2,4,8,16,32}
@@ -244,18 +248,36 @@ int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* p
 /* Y_i = alpha*A_i*X_i + beta*Y_i for every matrix of the batch: one kernel
  * launch, no allocation, no synchronization (capturable in a CUDA graph). */
 int merbit_batch_spmm(merbit_batch batch, double alpha, double beta, void* stream);
-/* Times the tile sizes and RHS vector widths the batch can use and keeps the
- * fastest (the autotuner's choice per batch signature).  Synchronizes. */
+/* The batch autotuner.  Times the SpMM kernel at each tile size and RHS
+ * vector width and, for k = 1 on 16-byte aligned arrays, the warp-tile
+ * kernel in each variant; with the warp-tile kernel it then chooses the
+ * items per lane (7, 11 or 15) per matrix signature class (mean row length
+ * and longest-row skew), largest classes first, keeping whatever times
+ * fastest for the whole launch.  The choices are cached per matrix
+ * signature.  Synchronizes. */
 int merbit_batch_tune(merbit_batch batch, void* stream);
 int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info);
+/* The configuration of matrix `index` of the batch (the reference fixes one
+ * VBLOCK/VSIGMA per build, CMakeLists.txt:4-6,22-25): the kernel (as in
+ * merbit_batch_info), its merge items per tile and items per lane.  With
+ * the warp-tile kernel (k = 1) each matrix has its own tile size, chosen by
+ * merbit_batch_tune per matrix signature class and cached per signature
+ * for later batches and plans of the process. */
+int merbit_batch_get_matrix_config(merbit_batch batch, int32_t index, int32_t* kernel,
+                                   int32_t* tile_items, int32_t* items_per_thread);
+/* Sets the items per lane (7, 11 or 15) of matrix `index` and switches the
+ * batch to the warp-tile kernel (k = 1 and 16-byte aligned arrays only,
+ * else MERBIT_ERR_UNSUPPORTED).  Synchronizes. */
+int merbit_batch_set_matrix_config(merbit_batch batch, int32_t index, int32_t items_per_thread,
+                                   void* stream);
 int merbit_batch_destroy(merbit_batch batch);
 
 /* y[nrow] = alpha*A*x + beta*y without allocating any device memory -- for
- * callers that cannot allocate on the call path: code running while a CUDA
- * stream is captured (cudaMalloc cannot be captured), hosts whose device
- * memory all belongs to their own pool allocator, and loops that cannot
- * afford cudaMalloc's implicit synchronization.  No counterpart in the
- * reference.
+ * callers that cannot allocate on the call path: hosts whose device memory
+ * all belongs to their own pool allocator (a framework's caching allocator
+ * that must not see a library take memory behind its back), and loops that
+ * cannot afford cudaMalloc's implicit synchronization.  No counterpart in
+ * the reference.
  *
  * Its scratch (tile coordinates, carry slots, launch counters) is one fixed
  * file-scope device array of about 1.3 MB, held by every GPU that loads the
@@ -264,13 +286,29 @@ int merbit_batch_destroy(merbit_batch batch);
  * rejected with MERBIT_ERR_INVALID -- use merbit_plan_create/merbit_spmv.
  * The caller passes all arrays (device pointers, same dtype rules as a
  * plan).  The structure is not validated: it must be valid CSR.  The first
- * call on a device looks the array up and initializes it on `stream`; make
- * that first call before any stream capture.  Every call reuses the same
- * array (each call rebuilds what it needs), so calls whose executions
- * overlap on the GPU -- on different streams without ordering -- race. */
+ * call on a device looks the array up, initializes it on `stream` and
+ * waits for that; make that first call before any stream capture (under
+ * capture it is refused with MERBIT_ERR_INVALID).  Every call reuses the
+ * same array (each call rebuilds what it needs), so calls whose executions
+ * overlap on the GPU -- on different streams without ordering -- race.
+ * A device-side wait that runs out is recorded, not returned (the call
+ * returns before the kernel runs): merbit_spmv_noalloc_check reports it,
+ * and it never carries over into the results of later calls. */
 int merbit_spmv_noalloc(int32_t nrow, int32_t ncol, int32_t nnz, const int32_t* d_row_ptr,
                         const int32_t* d_col_idx, const void* d_vals, merbit_dtype dtype,
                         double alpha, const void* d_x, double beta, void* d_y, void* stream);
+
+/* Device-side status of merbit_spmv_noalloc on the current device
+ * (MERBIT_ERR_TIMEOUT if a wait ran out in any call since the last check);
+ * reads and clears it on `stream`, allocates nothing, synchronizes `stream`.
+ * No counterpart in the reference. */
+int merbit_spmv_noalloc_check(void* stream);
+
+/* Failure-detection self-test of merbit_spmv_noalloc's scratch (no reference
+ * counterpart): as merbit_plan_selftest_wait, but the time-out is recorded
+ * in the no-allocation scratch of the current device, where
+ * merbit_spmv_noalloc_check reports it. */
+int merbit_spmv_noalloc_selftest_wait(int32_t which, int32_t wait_us, void* stream);
 
 /* Reads and clears the plan's device-side status (MERBIT_ERR_TIMEOUT if a
  * carry wait ran out in any launch since the last check).  Synchronizes. */

@@ -56,6 +56,7 @@ class _PlanInfo(C.Structure):
         ("num_tiles", C.c_int32), ("vectorized", C.c_int32), ("kind", C.c_int32),
         ("l1_carveout", C.c_int32), ("gather_l2_only", C.c_int32),
         ("metadata_bytes", C.c_int64), ("algorithmic_bytes", C.c_double),
+        ("max_row_len", C.c_int32),
     ]
 
 
@@ -94,9 +95,13 @@ SIGNATURES = {
     "merbit_batch_spmm": (C.c_int, [_P, C.c_double, C.c_double, _P]),
     "merbit_batch_tune": (C.c_int, [_P, _P]),
     "merbit_batch_get_info": (C.c_int, [_P, _P]),
+    "merbit_batch_get_matrix_config": (C.c_int, [_P, C.c_int32, _P, _P, _P]),
+    "merbit_batch_set_matrix_config": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
     "merbit_batch_destroy": (C.c_int, [_P]),
     "merbit_spmv_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int,
                                       C.c_double, _P, C.c_double, _P, _P]),
+    "merbit_spmv_noalloc_check": (C.c_int, [_P]),
+    "merbit_spmv_noalloc_selftest_wait": (C.c_int, [C.c_int32, C.c_int32, _P]),
     "merbit_status_string": (C.c_char_p, [C.c_int]),
     "merbit_last_cuda_error": (C.c_int, []),
     "merbit_last_error_detail": (C.c_char_p, []),
@@ -248,6 +253,7 @@ class PlanInfo:
     gather_l2_only: bool
     metadata_bytes: int
     algorithmic_bytes: float
+    max_row_len: int
 
 
 class Plan:
@@ -296,7 +302,8 @@ class Plan:
         _check(lib().merbit_plan_get_info(self._h, C.byref(i)))
         return PlanInfo(i.nrow, i.ncol, i.nnz, i.dtype, i.block, i.items_per_thread,
                         i.tile_items, i.num_tiles, bool(i.vectorized), i.kind, i.l1_carveout,
-                        bool(i.gather_l2_only), i.metadata_bytes, i.algorithmic_bytes)
+                        bool(i.gather_l2_only), i.metadata_bytes, i.algorithmic_bytes,
+                        i.max_row_len)
 
     def set_values(self, vals: torch.Tensor) -> None:
         _need_cuda(vals, "vals", self.vals.dtype)
@@ -403,7 +410,8 @@ class Plan:
 class _BatchInfo(C.Structure):
     _fields_ = [("count", C.c_int32), ("k", C.c_int32), ("dtype", C.c_int32),
                 ("tile_items", C.c_int32), ("vector_width", C.c_int32),
-                ("total_tiles", C.c_int32), ("nnz", C.c_int64), ("algorithmic_bytes", C.c_double)]
+                ("total_tiles", C.c_int32), ("nnz", C.c_int64), ("algorithmic_bytes", C.c_double),
+                ("kernel", C.c_int32), ("variant", C.c_int32)]
 
 
 class Batch:
@@ -442,6 +450,23 @@ class Batch:
         i = _BatchInfo()
         _check(lib().merbit_batch_get_info(self._h, C.byref(i)))
         return {f: getattr(i, f) for f, _ in _BatchInfo._fields_}
+
+    def matrix_configs(self) -> list[tuple[int, int, int]]:
+        """[(kernel, tile_items, items_per_thread)] of every matrix of the
+        batch (merbit_batch_get_matrix_config)."""
+        out = []
+        for i in range(len(self.plans)):
+            k, t, p = C.c_int32(), C.c_int32(), C.c_int32()
+            _check(lib().merbit_batch_get_matrix_config(self._h, i, C.byref(k), C.byref(t),
+                                                        C.byref(p)))
+            out.append((k.value, t.value, p.value))
+        return out
+
+    def set_matrix_config(self, index: int, items_per_thread: int, stream=None) -> None:
+        """Items per lane (7, 11, 15) of matrix `index` on the warp-tile
+        kernel (k = 1, aligned arrays)."""
+        _check(lib().merbit_batch_set_matrix_config(self._h, index, items_per_thread,
+                                                    _stream_ptr(stream)))
 
     def close(self) -> None:
         if self._h:

@@ -1,5 +1,6 @@
 // C ABI for the SpMM kernels (spmm.cu): one plan with k right-hand sides,
 // and batches of plans run by one persistent launch.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <map>
@@ -34,6 +35,7 @@ int alloc_spmm_slots(SpmmSlots* s, long long nslots, cudaStream_t st) {
 namespace {
 
 constexpr int kDefaultItems = 256;
+constexpr int kBatchDefaultIpt = 11;
 
 bool pow2(int k) { return k > 0 && (k & (k - 1)) == 0; }
 
@@ -69,6 +71,8 @@ SpmmDesc make_desc(merbit_plan_s* p, const Partition* part, const void* x, long 
     d.nnz = p->nnz;
     d.num_tiles = part->num_tiles;
     d.tile_begin = tile_begin;
+    d.ipt = 0;
+    d.pad = 0;
     return d;
 }
 
@@ -128,6 +132,12 @@ int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long 
 // Batch of plans sharing one persistent launch.
 struct merbit_batch_s {
     int count = 0, k = 0, dtype = 0, items = 256, vw = 1;
+    // kernel 0: the SpMM kernel (items, vw for every matrix); kernel 1 (k = 1,
+    // 16-byte aligned arrays): the warp-tile kernel with variant `variant`
+    // and ipt[i] items per lane for matrix i
+    int kernel = 0, variant = 0;
+    std::vector<int> ipt;
+    bool all_vec = true;
     int device = 0;
     std::vector<merbit_plan_s*> plans;
     std::vector<const void*> x;
@@ -144,6 +154,28 @@ using namespace merbit;
 
 namespace {
 
+// Uploads the descriptors and sizes the carry slots for `tot` tiles.
+int batch_upload(merbit_batch_s* b, const std::vector<SpmmDesc>& h, long long tot, cudaStream_t s) {
+    if (b->d_descs == nullptr) {
+        int st = dev_alloc(&b->d_descs, sizeof(SpmmDesc) * b->count, s);
+        if (st != MERBIT_OK) return st;
+    }
+    MERBIT_CUDA(cudaMemcpyAsync(b->d_descs, h.data(), sizeof(SpmmDesc) * b->count,
+                                cudaMemcpyHostToDevice, s));
+    if (b->slots.nslots < tot * b->k) {
+        if (b->slots.words) MERBIT_CUDA(cudaDeviceSynchronize());  // launches may use them
+        dev_free(b->slots.words, s);
+        dev_free(b->slots.state, s);
+        b->slots = SpmmSlots();
+        int st = alloc_spmm_slots(&b->slots, tot * b->k, s);
+        if (st != MERBIT_OK) return st;
+    }
+    MERBIT_CUDA(cudaStreamSynchronize(s));
+    b->total_tiles = (int)tot;
+    return MERBIT_OK;
+}
+
+// The SpMM kernel with `items` merge items per tile for every matrix.
 int batch_build(merbit_batch_s* b, int items, cudaStream_t s) {
     std::vector<SpmmDesc> h(b->count);
     long long tot = 0;
@@ -160,24 +192,33 @@ int batch_build(merbit_batch_s* b, int items, cudaStream_t s) {
     for (int i = 0; i < b->count; ++i)
         vw = std::min(vw, pick_vw(b->k, b->ldx[i], b->x[i], b->y[i], b->ldy[i], esz, items));
     if (!spmm_config_exists(b->k, vw, items)) vw = 1;
-    if (b->d_descs == nullptr) {
-        int st = dev_alloc(&b->d_descs, sizeof(SpmmDesc) * b->count, s);
-        if (st != MERBIT_OK) return st;
-    }
-    MERBIT_CUDA(cudaMemcpyAsync(b->d_descs, h.data(), sizeof(SpmmDesc) * b->count,
-                                cudaMemcpyHostToDevice, s));
-    if (b->slots.nslots < tot * b->k) {
-        if (b->slots.words) MERBIT_CUDA(cudaDeviceSynchronize());  // launches may use them
-        dev_free(b->slots.words, s);
-        dev_free(b->slots.state, s);
-        b->slots = SpmmSlots();
-        int st = alloc_spmm_slots(&b->slots, tot * b->k, s);
-        if (st != MERBIT_OK) return st;
-    }
-    MERBIT_CUDA(cudaStreamSynchronize(s));
+    int st = batch_upload(b, h, tot, s);
+    if (st != MERBIT_OK) return st;
+    b->kernel = 0;
     b->items = items;
     b->vw = vw;
-    b->total_tiles = (int)tot;
+    return MERBIT_OK;
+}
+
+// The warp-tile kernel (k = 1) with b->ipt[i] items per lane for matrix i.
+int batch_build_warp(merbit_batch_s* b, int variant, cudaStream_t s) {
+    std::vector<SpmmDesc> h(b->count);
+    long long tot = 0;
+    for (int i = 0; i < b->count; ++i) {
+        const Partition* part = nullptr;
+        int st = plan_partition(b->plans[i], 32 * b->ipt[i], &part, s);
+        if (st != MERBIT_OK) return st;
+        if (tot + part->num_tiles > INT_MAX) return fail(MERBIT_ERR_OVERFLOW, "batch: too many tiles");
+        h[i] = make_desc(b->plans[i], part, b->x[i], b->ldx[i], b->y[i], b->ldy[i], (int)tot);
+        h[i].ipt = b->ipt[i];
+        tot += part->num_tiles;
+    }
+    int st = batch_upload(b, h, tot, s);
+    if (st != MERBIT_OK) return st;
+    b->kernel = 1;
+    b->variant = variant;
+    b->items = 0;
+    b->vw = 1;
     return MERBIT_OK;
 }
 
@@ -192,7 +233,42 @@ int batch_run(merbit_batch_s* b, double alpha, double beta, cudaStream_t s) {
     a.total_tiles = b->total_tiles;
     a.alpha = alpha;
     a.beta = beta;
+    if (b->kernel == 1) return batch_warp_launch(b->dtype, b->variant, a, s);
     return spmm_launch(b->dtype, b->k, b->vw, b->items, a, s);
+}
+
+// Mean ms of one batch launch (2 warm-up launches, then `reps` timed).
+int time_batch(merbit_batch_s* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1, int reps,
+               float* ms) {
+    int st = MERBIT_OK;
+    for (int w = 0; w < 2 && st == MERBIT_OK; ++w) st = batch_run(b, 1.0, 0.0, s);
+    if (st != MERBIT_OK) return st;
+    MERBIT_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps && st == MERBIT_OK; ++r) st = batch_run(b, 1.0, 0.0, s);
+    if (st != MERBIT_OK) return st;
+    MERBIT_CUDA(cudaEventRecord(e1, s));
+    MERBIT_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    MERBIT_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    *ms = t / (float)reps;
+    return MERBIT_OK;
+}
+
+int log2_floor(double v) {
+    int b = 0;
+    while (v >= 2.0 && b < 62) {
+        v *= 0.5;
+        ++b;
+    }
+    return b;
+}
+
+// Signature class of a batch member for the per-class search of the items
+// per lane: mean row length and longest-row skew (both log2 buckets).
+int batch_class(const merbit_plan_s* p) {
+    const double mean = p->nrow > 0 ? (double)p->nnz / p->nrow : 0.0;
+    const double skew = p->max_row_len > 0 ? (double)p->max_row_len / std::max(mean, 1.0) : 1.0;
+    return log2_floor(mean + 1.0) * 64 + log2_floor(skew);
 }
 
 }  // namespace
@@ -264,6 +340,7 @@ int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* p
                                                 " is null, of another dtype, or has bad X/Y");
         }
         b->plans.push_back(p);
+        b->all_vec = b->all_vec && p->vec;
         b->x.push_back(d_x[i]);
         b->y.push_back(d_y[i]);
         b->ldx.push_back(ldx[i]);
@@ -272,7 +349,19 @@ int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* p
         b->algorithmic_bytes += 4.0 * (p->nrow + 1.0) + (double)p->nnz * (4.0 + (double)dtype_size(p->dtype)) +
                                 (double)k * (double)xy_size(p->dtype) * ((double)p->ncol + p->nrow);
     }
-    int st = batch_build(b, kDefaultItems, (cudaStream_t)stream);
+    // k = 1 on 16-byte aligned arrays: the warp-tile kernel, each matrix
+    // starting from the items per lane cached for its signature
+    int st;
+    if (k == 1 && b->all_vec) {
+        for (auto* p : b->plans) {
+            const int c = tune_cache_batch_ipt(p);
+            b->ipt.push_back(c > 0 ? c : kBatchDefaultIpt);
+        }
+        st = batch_build_warp(b, 0, (cudaStream_t)stream);
+    } else {
+        if (k == 1) b->ipt.assign(count, kBatchDefaultIpt);
+        st = batch_build(b, kDefaultItems, (cudaStream_t)stream);
+    }
     if (st != MERBIT_OK) {
         merbit_batch_destroy(b);
         return st;
@@ -289,14 +378,17 @@ int merbit_batch_spmm(merbit_batch batch, double alpha, double beta, void* strea
 int merbit_batch_tune(merbit_batch batch, void* stream) {
     if (!batch) return fail(MERBIT_ERR_INVALID, "batch_tune: batch is null");
     cudaStream_t s = (cudaStream_t)stream;
-    // candidates: tile items x widest legal vector width (narrower widths too)
-    const int items_c[2] = {256, 512};
-    int best_items = batch->items, best_vw = batch->vw;
-    float best = 1e30f;
     cudaEvent_t e0, e1;
     MERBIT_CUDA(cudaEventCreate(&e0));
     MERBIT_CUDA(cudaEventCreate(&e1));
     int st = MERBIT_OK;
+    // 1. the kernel: the SpMM kernel at each tile size and vector width,
+    //    and (k = 1, aligned arrays) the warp-tile kernel in each variant
+    //    with the current items per lane
+    int best_kernel = batch->kernel, best_items = batch->items, best_vw = batch->vw;
+    int best_variant = batch->variant;
+    float best = 1e30f;
+    const int items_c[2] = {256, 512};
     for (int ii = 0; ii < 2 && st == MERBIT_OK; ++ii) {
         st = batch_build(batch, items_c[ii], s);
         if (st != MERBIT_OK) break;
@@ -304,29 +396,99 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
         for (int vw = vmax; vw >= 1 && st == MERBIT_OK; vw >>= 1) {
             if (!spmm_config_exists(batch->k, vw, items_c[ii])) continue;
             batch->vw = vw;
-            for (int w = 0; w < 2 && st == MERBIT_OK; ++w) st = batch_run(batch, 1.0, 0.0, s);
-            cudaEventRecord(e0, s);
-            for (int r = 0; r < 3 && st == MERBIT_OK; ++r) st = batch_run(batch, 1.0, 0.0, s);
-            cudaEventRecord(e1, s);
-            if (cudaEventSynchronize(e1) != cudaSuccess) {
-                st = cuda_fail(cudaGetLastError(), "batch_tune");
-                break;
-            }
             float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best) {
+            st = time_batch(batch, s, e0, e1, 3, &ms);
+            if (st == MERBIT_OK && ms < best) {
                 best = ms;
+                best_kernel = 0;
                 best_items = items_c[ii];
                 best_vw = vw;
             }
         }
     }
+    const bool warp_ok = batch->k == 1 && batch->all_vec;
+    for (int v = 0; warp_ok && v < kBatchWarpVariants && st == MERBIT_OK; ++v) {
+        st = batch_build_warp(batch, v, s);
+        float ms = 0.f;
+        if (st == MERBIT_OK) st = time_batch(batch, s, e0, e1, 3, &ms);
+        if (st == MERBIT_OK && ms < best) {
+            best = ms;
+            best_kernel = 1;
+            best_variant = v;
+        }
+    }
+    // 2. warp-tile kernel: the items per lane per signature class, largest
+    //    classes first, one pass of coordinate descent over the classes
+    if (st == MERBIT_OK && best_kernel == 1) {
+        std::map<int, long long> class_nnz;
+        for (auto* p : batch->plans) class_nnz[batch_class(p)] += p->nnz;
+        std::vector<std::pair<long long, int>> order;
+        for (auto& kv : class_nnz) order.push_back({-kv.second, kv.first});
+        std::sort(order.begin(), order.end());
+        for (auto& oc : order) {
+            const int cls = oc.second;
+            std::vector<int> keep = batch->ipt;
+            int best_ipt = -1;
+            for (int c = 0; c < kNumBatchIpts && st == MERBIT_OK; ++c) {
+                for (int i = 0; i < batch->count; ++i)
+                    if (batch_class(batch->plans[i]) == cls) batch->ipt[i] = kBatchIpts[c];
+                st = batch_build_warp(batch, best_variant, s);
+                float ms = 0.f;
+                if (st == MERBIT_OK) st = time_batch(batch, s, e0, e1, 3, &ms);
+                if (st == MERBIT_OK && ms < best) {
+                    best = ms;
+                    best_ipt = kBatchIpts[c];
+                }
+            }
+            if (st != MERBIT_OK) break;
+            batch->ipt = keep;
+            if (best_ipt > 0)
+                for (int i = 0; i < batch->count; ++i)
+                    if (batch_class(batch->plans[i]) == cls) batch->ipt[i] = best_ipt;
+        }
+        if (st == MERBIT_OK)
+            for (int i = 0; i < batch->count; ++i)
+                tune_cache_store_batch_ipt(batch->plans[i], batch->ipt[i]);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != MERBIT_OK) return st;
+    if (best_kernel == 1) return batch_build_warp(batch, best_variant, s);
     st = batch_build(batch, best_items, s);
     if (st != MERBIT_OK) return st;
     batch->vw = best_vw;
+    return MERBIT_OK;
+}
+
+int merbit_batch_set_matrix_config(merbit_batch batch, int32_t index, int32_t items_per_thread,
+                                   void* stream) {
+    if (!batch) return fail(MERBIT_ERR_INVALID, "batch_set_matrix_config: batch is null");
+    if (index < 0 || index >= batch->count)
+        return fail(MERBIT_ERR_INVALID, "batch_set_matrix_config: index out of range");
+    if (batch->k != 1 || !batch->all_vec)
+        return fail(MERBIT_ERR_UNSUPPORTED,
+                    "batch_set_matrix_config: per-matrix tiles need k = 1 and 16-byte aligned arrays");
+    bool known = false;
+    for (int c = 0; c < kNumBatchIpts; ++c) known = known || kBatchIpts[c] == items_per_thread;
+    if (!known) return fail(MERBIT_ERR_INVALID, "batch_set_matrix_config: items_per_thread is 7, 11 or 15");
+    batch->ipt[index] = items_per_thread;
+    return batch_build_warp(batch, batch->kernel == 1 ? batch->variant : 0, (cudaStream_t)stream);
+}
+
+int merbit_batch_get_matrix_config(merbit_batch batch, int32_t index, int32_t* kernel,
+                                   int32_t* tile_items, int32_t* items_per_thread) {
+    if (!batch || !kernel || !tile_items || !items_per_thread)
+        return fail(MERBIT_ERR_INVALID, "batch_get_matrix_config: null pointer");
+    if (index < 0 || index >= batch->count)
+        return fail(MERBIT_ERR_INVALID, "batch_get_matrix_config: index out of range");
+    *kernel = batch->kernel;
+    if (batch->kernel == 1) {
+        *items_per_thread = batch->ipt[index];
+        *tile_items = 32 * batch->ipt[index];
+    } else {
+        *tile_items = batch->items;
+        *items_per_thread = batch->items / 32;
+    }
     return MERBIT_OK;
 }
 
@@ -340,6 +502,8 @@ int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info) {
     info->total_tiles = batch->total_tiles;
     info->nnz = batch->nnz;
     info->algorithmic_bytes = batch->algorithmic_bytes;
+    info->kernel = batch->kernel;
+    info->variant = batch->variant;
     return MERBIT_OK;
 }
 

@@ -194,16 +194,28 @@ int run_spmv(merbit_plan_s* p, int cfg, double alpha, const void* x, double beta
     return spmv_launch(p->dtype, cfg, p->vec, a, s);
 }
 
-// Tuning cache: matrix signature -> config index.
+// Tuning cache: matrix signature -> config index.  The signature buckets
+// (log2) the row count, the nonzero count, the density and the longest row,
+// so that a configuration tuned on short, even rows (a stencil, where the
+// row-group kernel wins) is never applied to a power-law matrix of the same
+// size, whose long rows serialize that kernel.
 struct Sig {
-    int dtype, vec, nrow_bucket, nnz_bucket, density_bucket;
-    bool operator<(const Sig& o) const {
-        return std::tie(dtype, vec, nrow_bucket, nnz_bucket, density_bucket) <
+    int dtype, vec, nrow_bucket, nnz_bucket, density_bucket, maxrow_bucket;
+    auto key() const {
+        return std::tie(dtype, vec, nrow_bucket, nnz_bucket, density_bucket, maxrow_bucket);
+    }
+    bool operator<(const Sig& o) const { return key() < o.key(); }
+    bool same_size(const Sig& o) const {
+        return std::tie(dtype, vec, nrow_bucket, nnz_bucket, density_bucket) ==
                std::tie(o.dtype, o.vec, o.nrow_bucket, o.nnz_bucket, o.density_bucket);
     }
 };
+struct Tuned {
+    int cfg;          // the configuration that won
+    int max_row_len;  // longest row of the matrix it was tuned on
+};
 std::mutex g_tune_mu;
-std::map<Sig, int> g_tune;
+std::map<Sig, Tuned> g_tune;
 
 int log2_bucket(double v) {
     int b = 0;
@@ -214,17 +226,56 @@ int log2_bucket(double v) {
     return b;
 }
 
-Sig signature(const merbit_plan_s* p) {
+Sig signature(const merbit_plan_s* p, int max_row_len) {
     Sig s;
     s.dtype = p->dtype;
     s.vec = p->vec;
     s.nrow_bucket = log2_bucket((double)p->nrow);
     s.nnz_bucket = log2_bucket((double)p->nnz);
     s.density_bucket = log2_bucket(4.0 * (double)p->nnz / (double)(p->nrow > 0 ? p->nrow : 1));
+    s.maxrow_bucket = log2_bucket((double)(max_row_len > 0 ? max_row_len : 0) + 1.0);
     return s;
 }
 
+// Whether a cached choice may serve a plan whose longest row is
+// max_row_len.  The row-group kernel gives each row to one lane group, so
+// its time grows with the longest row: it is kept only for matrices whose
+// longest row is at most twice the one it was tuned on.  Merge-path
+// kernels balance any row lengths and are checked by their rows-per-tile
+// cap instead.
+bool cached_choice_fits(int dtype, const Tuned& t, int max_row_len) {
+    if (spmv_config(dtype, t.cfg).kind != 3) return true;
+    return (long long)max_row_len <= 2LL * std::max(t.max_row_len, 1);
+}
+
+// Batched k = 1 warp-tile kernel: the items per lane the batch tuner chose
+// for a matrix signature (same signature as the SpMV tuner's).
+std::map<Sig, int> g_batch_ipt;
+
 }  // namespace
+
+int tune_cache_batch_ipt(const merbit_plan_s* p) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    const Sig sg = signature(p, p->max_row_len);
+    auto it = g_batch_ipt.find(sg);
+    if (it != g_batch_ipt.end()) return it->second;
+    // a warp-tile SpMV configuration tuned for this signature suggests its
+    // items per lane when the batch kernel has the same
+    auto jt = g_tune.find(sg);
+    if (jt != g_tune.end()) {
+        const SpmvConfig c = spmv_config(p->dtype, jt->second.cfg);
+        if (c.kind == 1)
+            for (int i = 0; i < kNumBatchIpts; ++i)
+                if (kBatchIpts[i] == c.ipt) return c.ipt;
+    }
+    return -1;
+}
+
+void tune_cache_store_batch_ipt(const merbit_plan_s* p, int ipt) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_batch_ipt[signature(p, p->max_row_len)] = ipt;
+}
+
 }  // namespace merbit
 
 using namespace merbit;
@@ -273,15 +324,22 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
     p->vals = d_vals;
     p->vec = aligned16(d_col_idx) && aligned16(d_vals) && aligned16(d_row_ptr);
     cudaGetDevice(&p->device);
-    int tuned = -1;
+    // A provisional choice before the longest row is known: a cached
+    // configuration of a matrix of the same size class (any longest-row
+    // bucket; the exact signature decides after the read-back below).
+    int provisional = -1;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        auto it = g_tune.find(signature(p));
-        if (it != g_tune.end()) tuned = it->second;
+        const Sig lo = signature(p, 0);
+        for (auto it = g_tune.lower_bound(lo); it != g_tune.end() && it->first.same_size(lo); ++it)
+            if (spmv_config(dtype, it->second.cfg).kind != 3) {
+                provisional = it->second.cfg;
+                break;
+            }
     }
     // one allocation for the launch state and the build's readback words;
-    // the whole build (validation, first partition, carry slots) is queued
-    // on s and read back with one synchronization
+    // the whole build (validation, longest row, first partition, carry
+    // slots) is queued on s and read back with one synchronization
     static_assert(sizeof(LaunchState) % alignof(PlanScratch) == 0, "scratch alignment");
     int st = dev_alloc(&p->state, sizeof(LaunchState) + sizeof(PlanScratch), s);
     if (st != MERBIT_OK) {
@@ -295,19 +353,19 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
     } init = {};
     static_assert(sizeof(init) == sizeof(LaunchState) + sizeof(PlanScratch), "state layout");
     init.ls.epoch = 1u;
-    init.sc = PlanScratch{0, {INT_MAX, INT_MAX}, 0};
+    init.sc = PlanScratch{0, {INT_MAX, INT_MAX}, 0, 0, 0};
     cudaError_t e = cudaMemcpyAsync(p->state, &init, sizeof(init), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
         merbit_plan_destroy(p);
         return cuda_fail(e, "plan_create: init state");
     }
     const bool validate = !(flags & MERBIT_PLAN_SKIP_VALIDATE);
-    st = validate ? validate_launch(d_row_ptr, d_col_idx, nrow, ncol, nnz, p->scratch, s)
-                  : MERBIT_OK;
-    // first candidate: the configuration tuned for this matrix signature,
-    // else the table's first entry the plan's alignment allows
+    st = validate_launch(d_row_ptr, d_col_idx, nrow, ncol, nnz, p->scratch, validate, s);
+    // first candidate: the provisional cached configuration, else the
+    // table's first entry the plan's alignment allows
     int first = -1;
-    if (tuned >= 0 && spmv_config_allowed(spmv_config(dtype, tuned), p->vec)) first = tuned;
+    if (provisional >= 0 && spmv_config_allowed(spmv_config(dtype, provisional), p->vec))
+        first = provisional;
     for (int i = 0, n = spmv_num_configs(dtype); first < 0 && i < n; ++i)
         if (spmv_config_allowed(spmv_config(dtype, i), p->vec)) first = i;
     Partition* part = nullptr;
@@ -321,13 +379,29 @@ int merbit_plan_create(merbit_plan* plan, int32_t nrow, int32_t ncol, int32_t nn
     }
     if (st == MERBIT_OK && validate) st = validate_status(h);
     if (st == MERBIT_OK) {
+        p->max_row_len = h.max_row_len;
         if (part) part->max_rows = h.max_rows;
-        const bool ok = first >= 0 && (!part || h.max_rows <= spmv_config_row_cap(
-                                                                   spmv_config(dtype, first)));
-        if (ok)
-            p->cfg = first;
-        else
-            st = plan_pick_default(p, s);  // reuses the partition built above
+        // the exact signature, longest row included
+        int tuned = -1;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = g_tune.find(signature(p, p->max_row_len));
+            if (it != g_tune.end() && cached_choice_fits(dtype, it->second, p->max_row_len))
+                tuned = it->second.cfg;
+        }
+        bool ok = false;
+        if (tuned >= 0) {
+            st = plan_config_ok(p, tuned, &ok, s);  // reuses the partition built above
+            if (st == MERBIT_OK && ok) p->cfg = tuned;
+        } else {
+            // no cached choice for this signature: the provisional one came
+            // from another longest-row bucket, so it is not kept
+            const bool from_cache = first == provisional && provisional >= 0;
+            ok = !from_cache && first >= 0 &&
+                 (!part || h.max_rows <= spmv_config_row_cap(spmv_config(dtype, first)));
+            if (ok) p->cfg = first;
+        }
+        if (st == MERBIT_OK && !ok) st = plan_pick_default(p, s);  // reuses built partitions
     }
     if (st != MERBIT_OK) {
         merbit_plan_destroy(p);
@@ -381,6 +455,7 @@ int merbit_plan_get_info(merbit_plan plan, merbit_plan_info* info) {
     info->l1_carveout = c.carveout;
     info->gather_l2_only = c.cg;
     info->metadata_bytes = meta;
+    info->max_row_len = plan->max_row_len;
     info->algorithmic_bytes = 4.0 * (plan->nrow + 1.0) +
                               (double)plan->nnz * (4.0 + (double)dtype_size(plan->dtype)) +
                               (double)xy_size(plan->dtype) * ((double)plan->ncol + plan->nrow);
@@ -467,7 +542,7 @@ int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream)
     if (st != MERBIT_OK) return st;
     plan->cfg = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[signature(plan)] = best;
+    g_tune[signature(plan, plan->max_row_len)] = Tuned{best, plan->max_row_len};
     return MERBIT_OK;
 }
 

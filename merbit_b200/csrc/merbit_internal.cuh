@@ -200,9 +200,11 @@ __device__ __forceinline__ void reset_other_parity(unsigned long long* slots, in
 // u-2, ... down to the tile that contains nonzero index rs (the start of
 // the row that tile u completes first), in a fixed order -- 32 tiles per
 // step, butterfly reduction -- so the result does not depend on timing.
+// Tile t's carry is in slot slot_base + t (a batch places each matrix's
+// tiles at its own offset of one slot array).
 __device__ __forceinline__ double look_back(const int2* coords, const unsigned long long* slots,
                                             int nslots, unsigned epoch, LaunchState* st, int u,
-                                            int rs, int lane) {
+                                            int rs, int lane, int slot_base = 0) {
     double total = 0.0;
     int base = u - 1;
     for (;;) {
@@ -212,7 +214,7 @@ __device__ __forceinline__ double look_back(const int2* coords, const unsigned l
         const unsigned m = __ballot_sync(0xFFFFFFFFu, !valid || cx <= rs);
         const int last = m ? __ffs(m) - 1 : 31;
         double c = 0.0;
-        if (valid && lane <= last) c = read_carry(slots, nslots, epoch, tq, st);
+        if (valid && lane <= last) c = read_carry(slots, nslots, epoch, slot_base + tq, st);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
         total += c;
@@ -374,13 +376,21 @@ struct PlanScratch {
     int err;
     int first_bad[2];
     int max_rows;
+    int max_row_len;  // longest row of the matrix
+    int pad;          // keeps the size a multiple of 8 (the state layout)
 };
 // Launches the structural CSR checks into sc->err / sc->first_bad (the
-// caller initializes them to 0 / INT_MAX); validate_status turns the words
-// read back into a status.
+// caller initializes them to 0 / INT_MAX) and the longest row into
+// sc->max_row_len (initialized to 0); with check == false only the longest
+// row is found.  validate_status turns the words read back into a status.
 int validate_launch(const int32_t* row_ptr, const int32_t* col, int nrow, int ncol, int nnz,
-                    PlanScratch* sc, cudaStream_t s);
+                    PlanScratch* sc, bool check, cudaStream_t s);
 int validate_status(const PlanScratch& h);
+
+// Failure-detection self-test: one bounded wait (which = 0 the carry wait,
+// 1 the mbarrier wait) on a flag nothing sets, recording its time-out in
+// *st (selftest.cu).
+int selftest_wait_on(LaunchState* st, int which, int wait_us, cudaStream_t s);
 
 // Carry / swap words of one SpMM slot family (2 parities x 2 arrays x
 // tiles x k) with its own launch state.
@@ -530,6 +540,8 @@ struct SpmmDesc {
     long long ldx, ldy;
     const int2* coords;
     int nrow, nnz, num_tiles, tile_begin;
+    int ipt;  // batched k = 1 warp-tile kernel: items per lane of this matrix's tiles
+    int pad;
 };
 
 struct SpmmLaunch {
@@ -554,6 +566,19 @@ struct SpmmLaunch {
 // Launches the SpMM kernel for k right-hand sides, vw values per lane and
 // `items` merge items per warp tile.
 int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s);
+
+// Batched warp-tile SpMV for k = 1 (batch_warp.cu): every descriptor's
+// tiles hold 32 * ipt merge items, ipt one of kBatchIpts; variant indexes
+// kBatchWarpVariants (gather hint and shared-memory carveout).
+constexpr int kBatchIpts[] = {7, 11, 15};
+constexpr int kNumBatchIpts = 3;
+constexpr int kBatchWarpVariants = 3;
+int batch_warp_launch(int dtype, int variant, const SpmmLaunch& a, cudaStream_t s);
+// The tuning cache, shared by merbit_plan_tune and merbit_batch_tune: the
+// items per lane of the batched k = 1 kernel for a plan's signature (-1:
+// nothing cached), and the store of a batch tuner's choice.
+int tune_cache_batch_ipt(const merbit_plan_s* p);
+void tune_cache_store_batch_ipt(const merbit_plan_s* p, int ipt);
 bool spmm_config_exists(int k, int vw, int items);
 
 }  // namespace merbit
@@ -567,6 +592,7 @@ struct merbit_plan_s {
     bool vec = false;
     int device = 0;
     int cfg = 0;  // index into the SpMV config table
+    int max_row_len = -1;  // longest row (-1: not measured)
     std::vector<merbit::Partition> parts;
     // carry slots shared by every launch of this plan (2 * slots words,
     // sized for the largest tile count in use)

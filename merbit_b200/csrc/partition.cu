@@ -103,18 +103,29 @@ __global__ void tile_build_kernel(const int32_t* __restrict__ row_ptr, int nrow,
 // of the decreasing / column checks.
 __global__ void validate_kernel(const int32_t* __restrict__ row_ptr,
                                 const int32_t* __restrict__ col, int nrow, int ncol, int nnz,
-                                int* __restrict__ err, int* __restrict__ first_bad) {
+                                int* __restrict__ err, int* __restrict__ first_bad,
+                                int* __restrict__ max_len, bool check) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i0 == 0) {
+    if (check && i0 == 0) {
         if (__ldg(row_ptr) != 0) atomicOr(err, 1);
         if (__ldg(row_ptr + nrow) != nnz) atomicOr(err, 2);
     }
-    for (long long i = i0; i < nrow; i += stride)
-        if (__ldg(row_ptr + i) > __ldg(row_ptr + i + 1)) {
-            atomicOr(err, 4);
-            atomicMin(first_bad, (int)i);
+    int longest = 0;
+    for (long long i = i0; i < nrow; i += stride) {
+        const int len = __ldg(row_ptr + i + 1) - __ldg(row_ptr + i);
+        if (len < 0) {
+            if (check) {
+                atomicOr(err, 4);
+                atomicMin(first_bad, (int)i);
+            }
+        } else {
+            longest = max(longest, len);
         }
+    }
+    for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xFFFFFFFFu, longest, o));
+    if ((threadIdx.x & 31) == 0 && longest > 0) atomicMax(max_len, longest);
+    if (!check) return;
     for (long long e = i0; e < nnz; e += stride) {
         const int c = __ldg(col + e);
         if (c < 0 || c >= ncol) {
@@ -160,12 +171,13 @@ int build_partition_async(const int32_t* row_ptr, int nrow, int nnz, int tile_it
 }
 
 int validate_launch(const int32_t* row_ptr, const int32_t* col, int nrow, int ncol, int nnz,
-                    PlanScratch* sc, cudaStream_t s) {
+                    PlanScratch* sc, bool check, cudaStream_t s) {
     int dev = 0, sms = 148;
     MERBIT_CUDA(cudaGetDevice(&dev));
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // blockDim a multiple of 32 and every thread reaches the warp reduction
     validate_kernel<<<sms * 8, 256, 0, s>>>(row_ptr, col, nrow, ncol, nnz, &sc->err,
-                                            sc->first_bad);
+                                            sc->first_bad, &sc->max_row_len, check);
     MERBIT_CUDA(cudaGetLastError());
     return MERBIT_OK;
 }

@@ -25,6 +25,17 @@ __global__ void mbar_wait_kernel(LaunchState* st, unsigned long long wait_ns) {
 }
 
 }  // namespace
+
+int selftest_wait_on(LaunchState* st, int which, int wait_us, cudaStream_t s) {
+    const unsigned long long ns = 1000ull * (unsigned long long)wait_us;
+    if (which == 0)
+        carry_wait_kernel<<<1, 32, 0, s>>>(st, ns);
+    else
+        mbar_wait_kernel<<<1, 32, 0, s>>>(st, ns);
+    MERBIT_CUDA(cudaGetLastError());
+    return MERBIT_OK;
+}
+
 }  // namespace merbit
 
 using namespace merbit;
@@ -36,12 +47,5 @@ extern "C" int merbit_plan_selftest_wait(merbit_plan plan, int32_t which, int32_
     if (wait_us < 1 || wait_us > 1000000)
         return fail(MERBIT_ERR_INVALID, "selftest_wait: wait_us outside [1, 1e6]");
     MERBIT_CUDA(cudaSetDevice(plan->device));
-    const unsigned long long ns = 1000ull * (unsigned long long)wait_us;
-    cudaStream_t s = (cudaStream_t)stream;
-    if (which == 0)
-        carry_wait_kernel<<<1, 32, 0, s>>>(plan->state, ns);
-    else
-        mbar_wait_kernel<<<1, 32, 0, s>>>(plan->state, ns);
-    MERBIT_CUDA(cudaGetLastError());
-    return MERBIT_OK;
+    return selftest_wait_on(plan->state, which, wait_us, (cudaStream_t)stream);
 }

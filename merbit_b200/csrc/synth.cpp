@@ -13,7 +13,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <parallel/algorithm>
 #include <vector>
 
 #include <omp.h>
@@ -232,8 +231,17 @@ int64_t merbit_synth_rmat(int64_t n, int64_t nedges, double a, double b, double 
     if (n <= 0 || nedges < 0 || n > INT32_MAX) return -1;
     int scale = 0;
     while (((int64_t)1 << scale) < n) ++scale;
-    std::vector<uint64_t> key((size_t)nedges);
-    const double ab = a + b, abc = a + b + c;
+    // 1. every edge draws its (row, col) from its own stream
+    std::vector<int32_t> er((size_t)nedges), ec((size_t)nedges);
+    // Quadrant choice per level from u = uniform() in [0,1): row bit u >= a+b,
+    // column bit a <= u < a+b or u >= a+b+c.  u is k * 2^-53 for the integer
+    // k = next() >> 11, so each comparison u >= t equals k >= ceil(t * 2^53)
+    // exactly; the integer form below draws the same bits without branches.
+    auto threshold = [](double t) {
+        const double s = std::ceil(t * 0x1.0p53);
+        return s <= 0.0 ? 0ull : (s >= 0x1.0p53 ? (1ull << 53) : (uint64_t)s);
+    };
+    const uint64_t ta = threshold(a), tab = threshold(a + b), tabc = threshold(a + b + c);
 #pragma omp parallel for schedule(static)
     for (int64_t e = 0; e < nedges; ++e) {
         Stream st(seed, kTagRmatEdge, (uint64_t)e);
@@ -242,28 +250,70 @@ int64_t merbit_synth_rmat(int64_t n, int64_t nedges, double a, double b, double 
             r = 0;
             q = 0;
             for (int l = 0; l < scale; ++l) {
-                const double u = st.uniform();
-                const uint64_t rb = u >= ab, cb = (u >= a && u < ab) || u >= abc;
+                const uint64_t k = st.next() >> 11;
+                const uint64_t rb = k >= tab;
+                const uint64_t cb = ((k >= ta) & (k < tab)) | (k >= tabc);
                 r = (r << 1) | rb;
                 q = (q << 1) | cb;
             }
         } while ((int64_t)r >= n || (int64_t)q >= n);
-        key[e] = (r << 32) | q;
+        er[e] = (int32_t)r;
+        ec[e] = (int32_t)q;
     }
-    __gnu_parallel::sort(key.begin(), key.end());
-    key.erase(std::unique(key.begin(), key.end()), key.end());
-    const int64_t nnz = (int64_t)key.size();
-    if (nnz > INT32_MAX) return -2;
-    // row_ptr by counting
-    std::vector<int64_t> cnt(n + 1, 0);
-    for (int64_t e = 0; e < nnz; ++e) cnt[(key[e] >> 32) + 1]++;
-    for (int64_t r = 0; r < n; ++r) cnt[r + 1] += cnt[r];
-    for (int64_t r = 0; r <= n; ++r) row_ptr[r] = (int32_t)cnt[r];
+    // 2. counting sort by row: per-chunk row histograms, then a scatter of
+    // the columns into row buckets (O(edges), no comparison sort)
+    const int nchunk = std::max(1, std::min(omp_get_max_threads(), 64));
+    std::vector<int64_t> hist((size_t)nchunk * (size_t)n, 0);
+    auto chunk_lo = [&](int t) { return nedges * t / nchunk; };
 #pragma omp parallel for schedule(static)
-    for (int64_t e = 0; e < nnz; ++e) {
-        col[e] = (int32_t)(key[e] & 0xFFFFFFFFull);
-        Stream sv(seed, kTagRmatVal, (uint64_t)e);
-        vals[e] = sv.normal();
+    for (int t = 0; t < nchunk; ++t) {
+        int64_t* h = hist.data() + (size_t)t * n;
+        for (int64_t e = chunk_lo(t); e < chunk_lo(t + 1); ++e) h[er[e]]++;
+    }
+    std::vector<int64_t> start((size_t)n + 1, 0);
+    for (int64_t r = 0; r < n; ++r) {
+        int64_t acc = start[r];
+        for (int t = 0; t < nchunk; ++t) {
+            const int64_t k = hist[(size_t)t * n + r];
+            hist[(size_t)t * n + r] = acc;  // this chunk's first slot in row r
+            acc += k;
+        }
+        start[r + 1] = acc;
+    }
+    std::vector<int32_t> bucket((size_t)nedges);
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < nchunk; ++t) {
+        int64_t* h = hist.data() + (size_t)t * n;
+        for (int64_t e = chunk_lo(t); e < chunk_lo(t + 1); ++e) bucket[h[er[e]]++] = ec[e];
+    }
+    std::vector<int32_t>().swap(er);
+    std::vector<int32_t>().swap(ec);
+    std::vector<int64_t>().swap(hist);
+    // 3. sort and de-duplicate the columns of each row
+    std::vector<int64_t> ulen((size_t)n);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t r = 0; r < n; ++r) {
+        int32_t* lo = bucket.data() + start[r];
+        int32_t* hi = bucket.data() + start[r + 1];
+        std::sort(lo, hi);
+        ulen[r] = std::unique(lo, hi) - lo;
+    }
+    int64_t nnz = 0;
+    for (int64_t r = 0; r < n; ++r) {
+        if (nnz > INT32_MAX) return -2;
+        row_ptr[r] = (int32_t)nnz;
+        nnz += ulen[r];
+    }
+    if (nnz > INT32_MAX) return -2;
+    row_ptr[n] = (int32_t)nnz;
+    // 4. compact into CSR; value e draws from stream e of the value tag
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t r = 0; r < n; ++r) {
+        std::memcpy(col + row_ptr[r], bucket.data() + start[r], sizeof(int32_t) * (size_t)ulen[r]);
+        for (int64_t e = row_ptr[r]; e < row_ptr[r + 1]; ++e) {
+            Stream sv(seed, kTagRmatVal, (uint64_t)e);
+            vals[e] = sv.normal();
+        }
     }
     return nnz;
 }

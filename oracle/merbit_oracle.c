@@ -284,6 +284,25 @@ int orc_spmv_omp_f64(int64_t nrow, const int32_t* row_ptr, const int32_t* col,
     return nthreads;
 }
 
+/* yabs[i] = sum_k |A[i,k]| |x[col_k]| in double, row-parallel: the
+ * denominator of the component-wise error for large matrices, where the
+ * extended-precision orc_spmm would take seconds.  Returns the threads used. */
+int orc_spmv_abs_omp_f64(int64_t nrow, const int32_t* row_ptr, const int32_t* col,
+                         const double* vals, const double* x, double* yabs, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads)
+    for (int64_t i = 0; i < nrow; ++i) {
+        double a = 0.0;
+        for (int64_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e) a += fabs(vals[e]) * fabs(x[col[e]]);
+        yabs[i] = a;
+    }
+    return nthreads;
+}
+
 /* Row-parallel OpenMP CSR SpMM in float (values f32, X/Y f32 row-major,
  * k columns, double accumulation per output): the CPU baseline of the
  * batched form.  Returns the number of threads used. */

@@ -63,6 +63,8 @@ def lib():
         L.orc_spmv_omp_f64.argtypes = [_i64, _p, _p, _p, _p, _p, C.c_int]
         L.orc_spmv_omp_f64.restype = C.c_int
         L.orc_max_threads.restype = C.c_int
+        L.orc_spmv_abs_omp_f64.argtypes = [_i64, _p, _p, _p, _p, _p, C.c_int]
+        L.orc_spmv_abs_omp_f64.restype = C.c_int
         L.orc_spmm_omp_f32.argtypes = [_i64, _p, _p, _p, _p, _i64, _p, C.c_int]
         L.orc_spmm_omp_f32.restype = C.c_int
         _lib = L
@@ -222,6 +224,18 @@ def spmv_omp_f64(row_ptr, col, vals, x, y=None, nthreads: int = 0):
     n = lib().orc_spmv_omp_f64(nrow, _ptr(row_ptr), _ptr(col), _ptr(vals), _ptr(x), _ptr(y),
                                nthreads)
     return y, n
+
+
+def spmv_abs_omp_f64(row_ptr, col, vals, x, nthreads: int = 0):
+    """sum_j |a_ij| |x_j| per row in double (OpenMP): the denominator of the
+    component-wise error for the full-size matrices."""
+    nrow = len(row_ptr) - 1
+    vals = np.ascontiguousarray(vals, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.empty(nrow, np.float64)
+    lib().orc_spmv_abs_omp_f64(nrow, _ptr(row_ptr), _ptr(col), _ptr(vals), _ptr(x), _ptr(y),
+                               nthreads)
+    return y
 
 
 def spmm_omp_f32(row_ptr, col, vals32, x32, k: int, y=None, nthreads: int = 0):

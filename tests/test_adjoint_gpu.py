@@ -69,17 +69,40 @@ def _diff_instance():
 
 
 @pytest.mark.gpu
-def test_gradcheck_fp64_finite_differences():
+def test_gradcheck_fp64_finite_differences_fast_mode():
+    """gradcheck on the whole 2,000-row instance (14,006 nonzeros, rows up
+    to 960 entries, i.e. spanning several merge-path tiles), with respect to
+    the values and X together.  Fast mode compares v^T J u for random u, v
+    against FP64 central differences, so every entry takes part."""
     A = _diff_instance()
-    # gradcheck perturbs every input entry: keep it to a slice of nonzeros
-    sub = csr_from_lengths(np.minimum(np.diff(A.row_ptr), 6)[:400], ncol=400, seed=7)
-    rp, col, v = to_cuda(sub, "f64")
-    M = SparseMatrix(rp, col, v.clone().requires_grad_(True))
-    X = torch.from_numpy(synth.uniform(2, sub.ncol * 3).reshape(sub.ncol, 3)).cuda()
+    assert A.nrow == 2000 and np.diff(A.row_ptr).max() > 512
+    rp, col, v = to_cuda(A, "f64")
+    vals = v.clone().requires_grad_(True)
+    M = SparseMatrix(rp, col, vals, ncol=A.ncol)
+    X = torch.from_numpy(synth.uniform(2, A.ncol * 3).reshape(A.ncol, 3)).cuda()
     X.requires_grad_(True)
-    vals = M.vals
     assert torch.autograd.gradcheck(lambda w, x: M.matmul(x, vals=w), (vals, X), eps=1e-6,
-                                    atol=1e-9, rtol=1e-7)
+                                    atol=1e-9, rtol=1e-7, fast_mode=True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("wrt", ["vals", "X"])
+def test_gradcheck_fp64_finite_differences_full_jacobian(wrt):
+    """The full Jacobian of the 2,000-row instance against FP64 central
+    differences, one input at a time: d Y / d vals (14,006 x 2,000, k = 1)
+    and d Y / d X (k = 2)."""
+    A = _diff_instance()
+    rp, col, v = to_cuda(A, "f64")
+    k = 1 if wrt == "vals" else 2
+    vals = v.clone().requires_grad_(wrt == "vals")
+    M = SparseMatrix(rp, col, vals, ncol=A.ncol)
+    X = torch.from_numpy(synth.uniform(2, A.ncol * k).reshape(A.ncol, k)).cuda()
+    X.requires_grad_(wrt == "X")
+    if wrt == "vals":
+        fn, inputs = (lambda w: M.matmul(X, vals=w)), (vals,)
+    else:
+        fn, inputs = (lambda x: M.matmul(x, vals=vals)), (X,)
+    assert torch.autograd.gradcheck(fn, inputs, eps=1e-6, atol=1e-9, rtol=1e-7)
 
 
 @pytest.mark.gpu
