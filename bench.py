@@ -450,6 +450,11 @@ def batch_forms(steps: int, dev, stream, peak: float, count: int = 128, ks=(1, 3
         batch = mb.Batch(p32, X32, Y32)
         batch.tune()
         binfo = batch.info()
+        per_matrix = {}
+        for kern, tile, ipt in batch.matrix_configs():
+            per_matrix[tile] = per_matrix.get(tile, 0) + 1
+        bkernel = (f"batch_warp_kernel variant {binfo['variant']}" if binfo["kernel"] == 1 else
+                   f"spmm_kernel vector_width={binfo['vector_width']}")
         batch.run()
         ms_b, clk_b = graph_time(lambda s: batch.run(stream=s), steps, dev, stream)
         # plain form: FP64 values, x and accumulation, one launch per matrix
@@ -497,8 +502,10 @@ def batch_forms(steps: int, dev, stream, peak: float, count: int = 128, ks=(1, 3
                 "roofline": {"bound": "hbm", "achieved": round(b32 / (ms_b * 1e-3) / 1e9, 2),
                              "peak": peak, "unit": "GB/s",
                              "frac": round(b32 / (ms_b * 1e-3) / 1e9 / peak, 4),
-                             "traffic": batch_traffic(k)},
-                "launches_per_step": 1, "tile_items": binfo["tile_items"],
+                             "traffic": batch_traffic(k),
+                             "kernel": bkernel.split()[0]},
+                "launches_per_step": 1, "kernel": bkernel,
+                "matrices_per_tile_items": {str(t): n for t, n in sorted(per_matrix.items())},
                 "vector_width": binfo["vector_width"], "clocks": clk_b,
                 "err_vs_plain_fp64": {"max": worst, "median": float(np.median(meds))},
             },
@@ -517,7 +524,7 @@ def batch_forms(steps: int, dev, stream, peak: float, count: int = 128, ks=(1, 3
 
 
 def batch_traffic(k: int):
-    p = os.path.join(ROOT, "profiles", f"spmm_f32_rmat128_k{k}_traffic.json")
+    p = os.path.join(ROOT, "profiles", f"batch_f32_rmat128_k{k}_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f).get("dram_bytes_per_launch")
@@ -942,6 +949,10 @@ def run_batch(args):
     if not args.no_tune:
         batch.tune()
     info = batch.info()
+    per_matrix = {}
+    for _, tile, _ in batch.matrix_configs():
+        per_matrix[str(tile)] = per_matrix.get(str(tile), 0) + 1
+    kname = "batch_warp_kernel" if info["kernel"] == 1 else "spmm_kernel"
     stream = torch.cuda.Stream(dev)
     stream.wait_stream(torch.cuda.current_stream(dev))
     graph = torch.cuda.CUDAGraph()
@@ -1003,16 +1014,18 @@ def run_batch(args):
         "data": "synthetic (seeded R-MAT generator, merbit_b200/synth.py)",
         "config": {"workload": f"rmat_batch{args.batch}", "matrices": len(mats), "k": k,
                    "nnz": int(info["nnz"]), "rows": int(sum(A.nrow for A in mats)),
-                   "tile_items": info["tile_items"], "vector_width": info["vector_width"],
-                   "launch": "one persistent kernel per step, CUDA-graph replay",
                    "l2": "inputs larger than L2"},
+        "launch": "one persistent kernel per step, CUDA-graph replay",
+        "kernel": f"{kname} variant={info['variant']} vector_width={info['vector_width']}",
+        "matrices_per_tile_items": per_matrix,
         "pct_hbm_peak": round(100.0 * achieved / peak, 2),
         "gflops": round(ws * 2.0 * info["nnz"] * k / (ms * 1e-3) / 1e9, 2),
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
-                     "peak_source": f"{peak_src} hbm_gbs (copy), burst", "traffic": None,
-                     "kernel": "spmm_kernel"},
+                     "peak_source": f"{peak_src} hbm_gbs (copy), burst",
+                     "traffic": batch_traffic(k) if args.batch == 128 else None,
+                     "kernel": kname},
         "e2e": {"value": round(ws * B / (ms_e2e * 1e-3) / 1e9, 2), "unit": "GB/s",
                 "h2d_bytes_per_step": int(sum(X.nbytes for X in xs)),
                 "d2h_bytes_per_step": int(sum(A.nrow * k * 4 for A in mats)),

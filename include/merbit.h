@@ -235,7 +235,11 @@ typedef struct merbit_batch_info {
     double algorithmic_bytes; /* sum over matrices of one SpMM's compulsory bytes */
     int32_t kernel;        /* 0: SpMM kernel (lane groups); 1: warp-tile kernel (k = 1) */
     int32_t variant;       /* kernel 1: 0 L1 gathers, all shared memory; 1 L1 gathers with a
-                              72% shared-memory carveout; 2 L2-only gathers, 72% carveout */
+                              72% shared-memory carveout; 2 L2-only gathers, 72% carveout;
+                              5 L1 gathers, 58% carveout (these take 7, 11 or 15 items per
+                              lane); 3 and 4 as 0 and 1 with stages for 15, 19 or 23 items
+                              per lane; 6 and 7 as 5 and 1 with stages for 7 or 11; 8 as 6
+                              with a 44% carveout; 9 as 6 with CTAs of 4 warps */
 } merbit_batch_info;
 
 /* A batch of `count` plans (same dtype) multiplied by k in {1,2,4,8,16,32}
@@ -265,9 +269,18 @@ int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info);
  * for later batches and plans of the process. */
 int merbit_batch_get_matrix_config(merbit_batch batch, int32_t index, int32_t* kernel,
                                    int32_t* tile_items, int32_t* items_per_thread);
-/* Sets the items per lane (7, 11 or 15) of matrix `index` and switches the
- * batch to the warp-tile kernel (k = 1 and 16-byte aligned arrays only,
- * else MERBIT_ERR_UNSUPPORTED).  Synchronizes. */
+/* Selects the batch's kernel by hand (as merbit_plan_set_config does for a
+ * plan): kernel 0, the SpMM kernel with `option` merge items per tile (256
+ * or 512; with vector width 4 also tiles of an odd number of items per lane
+ * group: 288/480 for k = 1 or 4, 272/496 for k = 8, 264/504 for k = 16,
+ * 260/508 for k = 32; widest legal vector width); kernel 1, the warp-tile kernel (k = 1,
+ * 16-byte aligned arrays) in variant `option` (0-9, see merbit_batch_info).
+ * Synchronizes. */
+int merbit_batch_set_kernel(merbit_batch batch, int32_t kernel, int32_t option, void* stream);
+/* Sets the items per lane of matrix `index` -- one the kernel variant in use
+ * takes (see merbit_batch_info) -- and
+ * switches the batch to the warp-tile kernel (k = 1 and 16-byte aligned
+ * arrays only, else MERBIT_ERR_UNSUPPORTED).  Synchronizes. */
 int merbit_batch_set_matrix_config(merbit_batch batch, int32_t index, int32_t items_per_thread,
                                    void* stream);
 int merbit_batch_destroy(merbit_batch batch);

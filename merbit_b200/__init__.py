@@ -97,6 +97,7 @@ SIGNATURES = {
     "merbit_batch_get_info": (C.c_int, [_P, _P]),
     "merbit_batch_get_matrix_config": (C.c_int, [_P, C.c_int32, _P, _P, _P]),
     "merbit_batch_set_matrix_config": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
+    "merbit_batch_set_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
     "merbit_batch_destroy": (C.c_int, [_P]),
     "merbit_spmv_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int,
                                       C.c_double, _P, C.c_double, _P, _P]),
@@ -461,6 +462,11 @@ class Batch:
                                                         C.byref(p)))
             out.append((k.value, t.value, p.value))
         return out
+
+    def set_kernel(self, kernel: int, option: int, stream=None) -> None:
+        """kernel 0: SpMM kernel with `option` (256/512) items per tile;
+        kernel 1: warp-tile kernel (k = 1) in variant `option` (0-2)."""
+        _check(lib().merbit_batch_set_kernel(self._h, kernel, option, _stream_ptr(stream)))
 
     def set_matrix_config(self, index: int, items_per_thread: int, stream=None) -> None:
         """Items per lane (7, 11, 15) of matrix `index` on the warp-tile

@@ -36,6 +36,7 @@ namespace {
 
 constexpr int kDefaultItems = 256;
 constexpr int kBatchDefaultIpt = 11;
+constexpr int kBatchDefaultVariant = 6;
 
 bool pow2(int k) { return k > 0 && (k & (k - 1)) == 0; }
 
@@ -200,11 +201,18 @@ int batch_build(merbit_batch_s* b, int items, cudaStream_t s) {
     return MERBIT_OK;
 }
 
-// The warp-tile kernel (k = 1) with b->ipt[i] items per lane for matrix i.
+// Nearest items per lane that `variant` takes.
+int ipt_for_variant(int variant, int ipt) {
+    return batch_variant_takes(variant, ipt) ? ipt : batch_variant_start_ipt(variant);
+}
+
+// The warp-tile kernel (k = 1) with b->ipt[i] items per lane for matrix i
+// (items per lane the variant does not take become its starting value).
 int batch_build_warp(merbit_batch_s* b, int variant, cudaStream_t s) {
     std::vector<SpmmDesc> h(b->count);
     long long tot = 0;
     for (int i = 0; i < b->count; ++i) {
+        b->ipt[i] = ipt_for_variant(variant, b->ipt[i]);
         const Partition* part = nullptr;
         int st = plan_partition(b->plans[i], 32 * b->ipt[i], &part, s);
         if (st != MERBIT_OK) return st;
@@ -349,15 +357,26 @@ int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* p
         b->algorithmic_bytes += 4.0 * (p->nrow + 1.0) + (double)p->nnz * (4.0 + (double)dtype_size(p->dtype)) +
                                 (double)k * (double)xy_size(p->dtype) * ((double)p->ncol + p->nrow);
     }
-    // k = 1 on 16-byte aligned arrays: the warp-tile kernel, each matrix
-    // starting from the items per lane cached for its signature
+    // k = 1 on 16-byte aligned arrays: the warp-tile kernel in the variant
+    // that measured fastest on the R-MAT batch (58% carveout, stages for 11
+    // items per lane), each matrix starting from the items per lane cached
+    // for its signature
+    // (and the variant they were tuned in, when every cached member agrees)
     int st;
     if (k == 1 && b->all_vec) {
+        int variant = -1;
+        bool agree = true;
         for (auto* p : b->plans) {
-            const int c = tune_cache_batch_ipt(p);
+            int v = -1;
+            const int c = tune_cache_batch_ipt(p, &v);
             b->ipt.push_back(c > 0 ? c : kBatchDefaultIpt);
+            if (v >= 0) {
+                agree = agree && (variant < 0 || variant == v);
+                variant = v;
+            }
         }
-        st = batch_build_warp(b, 0, (cudaStream_t)stream);
+        if (variant < 0 || !agree) variant = kBatchDefaultVariant;
+        st = batch_build_warp(b, variant, (cudaStream_t)stream);
     } else {
         if (k == 1) b->ipt.assign(count, kBatchDefaultIpt);
         st = batch_build(b, kDefaultItems, (cudaStream_t)stream);
@@ -388,8 +407,9 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
     int best_kernel = batch->kernel, best_items = batch->items, best_vw = batch->vw;
     int best_variant = batch->variant;
     float best = 1e30f;
-    const int items_c[2] = {256, 512};
-    for (int ii = 0; ii < 2 && st == MERBIT_OK; ++ii) {
+    int items_c[4];
+    const int nitems = spmm_tile_candidates(batch->k, items_c);
+    for (int ii = 0; ii < nitems && st == MERBIT_OK; ++ii) {
         st = batch_build(batch, items_c[ii], s);
         if (st != MERBIT_OK) break;
         const int vmax = batch->vw;
@@ -406,8 +426,11 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
             }
         }
     }
+    // the warp-tile kernel's variants, every matrix at the variant's
+    // starting items per lane
     const bool warp_ok = batch->k == 1 && batch->all_vec;
     for (int v = 0; warp_ok && v < kBatchWarpVariants && st == MERBIT_OK; ++v) {
+        batch->ipt.assign(batch->count, batch_variant_start_ipt(v));
         st = batch_build_warp(batch, v, s);
         float ms = 0.f;
         if (st == MERBIT_OK) st = time_batch(batch, s, e0, e1, 3, &ms);
@@ -417,6 +440,7 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
             best_variant = v;
         }
     }
+    if (warp_ok) batch->ipt.assign(batch->count, batch_variant_start_ipt(best_variant));
     // 2. warp-tile kernel: the items per lane per signature class, largest
     //    classes first, one pass of coordinate descent over the classes
     if (st == MERBIT_OK && best_kernel == 1) {
@@ -430,6 +454,7 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
             std::vector<int> keep = batch->ipt;
             int best_ipt = -1;
             for (int c = 0; c < kNumBatchIpts && st == MERBIT_OK; ++c) {
+                if (!batch_variant_takes(best_variant, kBatchIpts[c])) continue;
                 for (int i = 0; i < batch->count; ++i)
                     if (batch_class(batch->plans[i]) == cls) batch->ipt[i] = kBatchIpts[c];
                 st = batch_build_warp(batch, best_variant, s);
@@ -448,7 +473,7 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
         }
         if (st == MERBIT_OK)
             for (int i = 0; i < batch->count; ++i)
-                tune_cache_store_batch_ipt(batch->plans[i], batch->ipt[i]);
+                tune_cache_store_batch_ipt(batch->plans[i], best_variant, batch->ipt[i]);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -460,6 +485,29 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
     return MERBIT_OK;
 }
 
+int merbit_batch_set_kernel(merbit_batch batch, int32_t kernel, int32_t option, void* stream) {
+    if (!batch) return fail(MERBIT_ERR_INVALID, "batch_set_kernel: batch is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (kernel == 0) {
+        int cand[4];
+        const int n = spmm_tile_candidates(batch->k, cand);
+        bool known = false;
+        for (int i = 0; i < n; ++i) known = known || cand[i] == option;
+        if (!known)
+            return fail(MERBIT_ERR_INVALID, "batch_set_kernel: no SpMM tile of that size for this k");
+        return batch_build(batch, option, s);
+    }
+    if (kernel == 1) {
+        if (batch->k != 1 || !batch->all_vec)
+            return fail(MERBIT_ERR_UNSUPPORTED,
+                        "batch_set_kernel: the warp-tile kernel needs k = 1 and 16-byte aligned arrays");
+        if (option < 0 || option >= kBatchWarpVariants)
+            return fail(MERBIT_ERR_INVALID, "batch_set_kernel: no such variant");
+        return batch_build_warp(batch, option, s);
+    }
+    return fail(MERBIT_ERR_INVALID, "batch_set_kernel: kernel is 0 or 1");
+}
+
 int merbit_batch_set_matrix_config(merbit_batch batch, int32_t index, int32_t items_per_thread,
                                    void* stream) {
     if (!batch) return fail(MERBIT_ERR_INVALID, "batch_set_matrix_config: batch is null");
@@ -468,11 +516,14 @@ int merbit_batch_set_matrix_config(merbit_batch batch, int32_t index, int32_t it
     if (batch->k != 1 || !batch->all_vec)
         return fail(MERBIT_ERR_UNSUPPORTED,
                     "batch_set_matrix_config: per-matrix tiles need k = 1 and 16-byte aligned arrays");
-    bool known = false;
-    for (int c = 0; c < kNumBatchIpts; ++c) known = known || kBatchIpts[c] == items_per_thread;
-    if (!known) return fail(MERBIT_ERR_INVALID, "batch_set_matrix_config: items_per_thread is 7, 11 or 15");
+    const int variant = batch->kernel == 1 ? batch->variant : 0;
+    if (!batch_variant_takes(variant, items_per_thread))
+        return fail(MERBIT_ERR_INVALID,
+                    "batch_set_matrix_config: the kernel variant in use does not take that many "
+                    "items per lane (variants 0-2 and 5: 7, 11, 15; 3-4: 15, 19, 23; 6-9: 7, 11); "
+                    "select the variant first with merbit_batch_set_kernel");
     batch->ipt[index] = items_per_thread;
-    return batch_build_warp(batch, batch->kernel == 1 ? batch->variant : 0, (cudaStream_t)stream);
+    return batch_build_warp(batch, variant, (cudaStream_t)stream);
 }
 
 int merbit_batch_get_matrix_config(merbit_batch batch, int32_t index, int32_t* kernel,

@@ -15,11 +15,12 @@
 // tiles.  Results are bitwise those of the single-matrix warp-tile kernel
 // with the same items per lane.
 //
-// Per matrix: the items per lane (7, 11 or 15; tile = 32 x ipt items) is a
-// property of the matrix's descriptor, chosen by the batch tuner per matrix
-// signature.  One stage per warp is sized for the largest tile, with a
-// row_ptr window for a tile whose every item ends a row, so no member is
-// restricted in rows per tile (R-MAT matrices have runs of empty rows).
+// Per matrix: the items per lane (7, 11, 15, 19 or 23; tile = 32 x ipt
+// items) is a property of the matrix's descriptor, chosen by the batch tuner
+// per matrix signature.  One stage per warp is sized for the largest tile
+// of the kernel variant (11, 15 or 23 items per lane), with a row_ptr window
+// for a tile whose every item ends a row, so no member is restricted in
+// rows per tile (R-MAT matrices have runs of empty rows).
 //
 // When a warp moves on to another matrix it first finishes what it holds
 // of the previous one: its pending boundary swaps and its queued look-backs
@@ -33,12 +34,11 @@ namespace merbit {
 
 namespace {
 
-constexpr int kBatchMaxIpt = 15;
 constexpr int kBatchWarps = 8;
 
-template <int DT>
-using BatchSmem = WarpSmem<typename Prec<DT>::V, typename Prec<DT>::P, kBatchMaxIpt,
-                           32 * kBatchMaxIpt + 16>;
+// One stage for tiles of up to 32 * MAXIPT items, every item possibly a row end.
+template <int DT, int MAXIPT>
+using BatchSmem = WarpSmem<typename Prec<DT>::V, typename Prec<DT>::P, MAXIPT, 32 * MAXIPT + 16>;
 
 // Tile source of a batch member: its descriptor, copied to the warp's
 // shared memory when the warp reaches the matrix.
@@ -74,12 +74,46 @@ struct BatchRowStore {
     }
 };
 
-template <int DT, bool CG, int IPT>
-using BT = WarpTile<DT, IPT, CG, BatchSmem<DT>>;
+template <int DT, bool CG, int IPT, int MAXIPT>
+using BT = WarpTile<DT, IPT, CG, BatchSmem<DT, MAXIPT>>;
 
-template <int DT, int WARPS, bool CG, int CV>
+// Issues (ISSUE) or processes the tile of `ipt` items per lane: a kernel
+// with stages for MAXIPT takes ipt in {7, 11} (11), {7, 11, 15} (15) or
+// {15, 19, 23} (23); the tuner only assigns those.
+template <int DT, bool CG, int MAXIPT, bool ISSUE, int IPT, class... A>
+__device__ __forceinline__ void run_ipt(A&&... args) {
+    if constexpr (ISSUE)
+        BT<DT, CG, IPT, MAXIPT>::issue(args...);
+    else
+        BT<DT, CG, IPT, MAXIPT>::process(args...);
+}
+template <int DT, bool CG, int MAXIPT, bool ISSUE, class... A>
+__device__ __forceinline__ void dispatch_ipt(int ipt, A&&... args) {
+    if constexpr (MAXIPT == 11) {
+        if (ipt == 7)
+            run_ipt<DT, CG, MAXIPT, ISSUE, 7>(args...);
+        else
+            run_ipt<DT, CG, MAXIPT, ISSUE, 11>(args...);
+    } else if constexpr (MAXIPT == 15) {
+        if (ipt == 7)
+            run_ipt<DT, CG, MAXIPT, ISSUE, 7>(args...);
+        else if (ipt == 11)
+            run_ipt<DT, CG, MAXIPT, ISSUE, 11>(args...);
+        else
+            run_ipt<DT, CG, MAXIPT, ISSUE, 15>(args...);
+    } else {
+        if (ipt == 15)
+            run_ipt<DT, CG, MAXIPT, ISSUE, 15>(args...);
+        else if (ipt == 19)
+            run_ipt<DT, CG, MAXIPT, ISSUE, 19>(args...);
+        else
+            run_ipt<DT, CG, MAXIPT, ISSUE, 23>(args...);
+    }
+}
+
+template <int DT, int WARPS, bool CG, int CV, int MAXIPT>
 __global__ void __launch_bounds__(WARPS * 32) batch_warp_kernel(const SpmmLaunch a) {
-    using S = BatchSmem<DT>;
+    using S = BatchSmem<DT, MAXIPT>;
     using Y = typename Prec<DT>::Y;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned s_epoch;
@@ -132,23 +166,13 @@ __global__ void __launch_bounds__(WARPS * 32) batch_warp_kernel(const SpmmLaunch
         }
         const int lt = u - s_desc[warp].tile_begin;
         const int ipt = s_desc[warp].ipt;  // warp-uniform
-        if (ipt == 7)
-            BT<DT, CG, 7>::issue(src, lt, ws, bar, lane);
-        else if (ipt == 11)
-            BT<DT, CG, 11>::issue(src, lt, ws, bar, lane);
-        else
-            BT<DT, CG, 15>::issue(src, lt, ws, bar, lane);
+        dispatch_ipt<DT, CG, MAXIPT, true>(ipt, src, lt, ws, bar, lane);
         const bool ok = __all_sync(0xFFFFFFFFu, mbar_wait_bounded(bar, phase, a.state));
         phase ^= 1u;
         __syncwarp();
-        if (ok) {
-            if (ipt == 7)
-                BT<DT, CG, 7>::process(src, lt, epoch, ws, lane, pa, pb, out, s_lbq[warp], nlb);
-            else if (ipt == 11)
-                BT<DT, CG, 11>::process(src, lt, epoch, ws, lane, pa, pb, out, s_lbq[warp], nlb);
-            else
-                BT<DT, CG, 15>::process(src, lt, epoch, ws, lane, pa, pb, out, s_lbq[warp], nlb);
-        }
+        if (ok)
+            dispatch_ipt<DT, CG, MAXIPT, false>(ipt, src, lt, epoch, ws, lane, pa, pb, out,
+                                                s_lbq[warp], nlb);
     }
     if (m >= 0) {
         resolve_swap(pa, out);
@@ -160,13 +184,13 @@ __global__ void __launch_bounds__(WARPS * 32) batch_warp_kernel(const SpmmLaunch
 }
 
 // Persistent cooperative grid of batch_warp_kernel (all CTAs resident).
-template <int DT, bool CG, int CV>
+template <int DT, bool CG, int CV, int MAXIPT, int WARPS = kBatchWarps>
 int launch_batch_warp(const SpmmLaunch& a, cudaStream_t s) {
-    using S = BatchSmem<DT>;
-    constexpr size_t smem = S::bytes * kBatchWarps;
+    using S = BatchSmem<DT, MAXIPT>;
+    constexpr size_t smem = S::bytes * WARPS;
     static int grid_cap[64] = {};
     static std::mutex mu;
-    auto kern = batch_warp_kernel<DT, kBatchWarps, CG, CV>;
+    auto kern = batch_warp_kernel<DT, WARPS, CG, CV, MAXIPT>;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "batch_warp: device ordinal >= 64");
@@ -181,17 +205,17 @@ int launch_batch_warp(const SpmmLaunch& a, cudaStream_t s) {
             if (e != cudaSuccess) return cuda_fail(e, "batch_warp_kernel carveout");
         }
         int per_sm = 0, sms = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchWarps * 32, smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem);
         if (e != cudaSuccess) return cuda_fail(e, "occupancy(batch_warp_kernel)");
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cap = per_sm > 0 && sms > 0 ? per_sm * sms : 1;
         __atomic_store_n(&grid_cap[dev], cap, __ATOMIC_RELEASE);
     }
-    const long long need = ((long long)a.total_tiles + kBatchWarps - 1) / kBatchWarps;
+    const long long need = ((long long)a.total_tiles + WARPS - 1) / WARPS;
     const int grid = (int)(need < cap ? need : cap);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3(kBatchWarps * 32);
+    cfg.blockDim = dim3(WARPS * 32);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[2];
@@ -212,9 +236,16 @@ int launch_batch_warp(const SpmmLaunch& a, cudaStream_t s) {
 template <int DT>
 int launch_batch_warp_dt(int variant, const SpmmLaunch& a, cudaStream_t s) {
     switch (variant) {
-    case 0: return launch_batch_warp<DT, false, 0>(a, s);            // L1 gathers, all shared
-    case 1: return launch_batch_warp<DT, false, kCarveoutL1>(a, s);  // L1 gathers, more L1
-    case 2: return launch_batch_warp<DT, true, kCarveoutL1>(a, s);   // L2-only gathers
+    case 0: return launch_batch_warp<DT, false, 0, 15>(a, s);            // L1 gathers, all shared
+    case 1: return launch_batch_warp<DT, false, kCarveoutL1, 15>(a, s);  // L1 gathers, more L1
+    case 2: return launch_batch_warp<DT, true, kCarveoutL1, 15>(a, s);   // L2-only gathers
+    case 3: return launch_batch_warp<DT, false, 0, 23>(a, s);            // larger tiles
+    case 4: return launch_batch_warp<DT, false, kCarveoutL1, 23>(a, s);
+    case 5: return launch_batch_warp<DT, false, kCarveoutL1Max, 15>(a, s);  // still more L1
+    case 6: return launch_batch_warp<DT, false, kCarveoutL1Max, 11>(a, s);  // smaller stages
+    case 7: return launch_batch_warp<DT, false, kCarveoutL1, 11>(a, s);
+    case 8: return launch_batch_warp<DT, false, kCarveoutL1Most, 11>(a, s);  // most L1
+    case 9: return launch_batch_warp<DT, false, kCarveoutL1Max, 11, 4>(a, s);  // 4-warp CTAs
     }
     return fail(MERBIT_ERR_INVALID, "batch_warp: no such variant");
 }

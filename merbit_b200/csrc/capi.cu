@@ -248,17 +248,21 @@ bool cached_choice_fits(int dtype, const Tuned& t, int max_row_len) {
     return (long long)max_row_len <= 2LL * std::max(t.max_row_len, 1);
 }
 
-// Batched k = 1 warp-tile kernel: the items per lane the batch tuner chose
-// for a matrix signature (same signature as the SpMV tuner's).
-std::map<Sig, int> g_batch_ipt;
+// Batched k = 1 warp-tile kernel: the (variant, items per lane) the batch
+// tuner chose for a matrix signature (same signature as the SpMV tuner's).
+std::map<Sig, std::pair<int, int>> g_batch_ipt;
 
 }  // namespace
 
-int tune_cache_batch_ipt(const merbit_plan_s* p) {
+int tune_cache_batch_ipt(const merbit_plan_s* p, int* variant) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     const Sig sg = signature(p, p->max_row_len);
+    *variant = -1;
     auto it = g_batch_ipt.find(sg);
-    if (it != g_batch_ipt.end()) return it->second;
+    if (it != g_batch_ipt.end()) {
+        *variant = it->second.first;
+        return it->second.second;
+    }
     // a warp-tile SpMV configuration tuned for this signature suggests its
     // items per lane when the batch kernel has the same
     auto jt = g_tune.find(sg);
@@ -271,9 +275,9 @@ int tune_cache_batch_ipt(const merbit_plan_s* p) {
     return -1;
 }
 
-void tune_cache_store_batch_ipt(const merbit_plan_s* p, int ipt) {
+void tune_cache_store_batch_ipt(const merbit_plan_s* p, int variant, int ipt) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_batch_ipt[signature(p, p->max_row_len)] = ipt;
+    g_batch_ipt[signature(p, p->max_row_len)] = {variant, ipt};
 }
 
 }  // namespace merbit

@@ -416,11 +416,14 @@ struct SpmvConfig {
     int cg;  // 1: x gathers cached in L2 only (ld.global.cg)
     // Row-group kernel: 1 = a warp loads its row block's nonzeros as one
     // contiguous run (coalesced) and stages the products in shared memory
-    // for the groups to reduce; 0 = each group reads its own row strided
+    // for the groups to reduce; 0 = each group reads its own row strided.
+    // Warp-tile kernel: 1 = the row_ptr window holds a tile whose every item
+    // ends a row (no cap on rows per tile), 0 = warp_rp_cap(ipt) entries.
     int stg;
 };
 constexpr int kCarveoutL1 = 72;     // ~164 KB shared memory, the rest L1
 constexpr int kCarveoutL1Max = 58;  // ~132 KB shared memory
+constexpr int kCarveoutL1Most = 44;  // ~100 KB shared memory
 int spmv_num_configs(int dtype);
 SpmvConfig spmv_config(int dtype, int idx);
 int spmv_tile_items(const SpmvConfig& c);
@@ -569,17 +572,36 @@ int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaSt
 
 // Batched warp-tile SpMV for k = 1 (batch_warp.cu): every descriptor's
 // tiles hold 32 * ipt merge items, ipt one of kBatchIpts; variant indexes
-// kBatchWarpVariants (gather hint and shared-memory carveout).
-constexpr int kBatchIpts[] = {7, 11, 15};
-constexpr int kNumBatchIpts = 3;
-constexpr int kBatchWarpVariants = 3;
+// kBatchWarpVariants: gather hint, shared-memory carveout and the largest
+// tile its stages hold (11, 15 or 23 items per lane).  A variant takes the
+// items per lane up to its largest, from {7, 11, 15} or {15, 19, 23}.
+constexpr int kBatchIpts[] = {7, 11, 15, 19, 23};
+constexpr int kNumBatchIpts = 5;
+constexpr int kBatchWarpVariants = 10;
+constexpr int batch_variant_max_ipt(int variant) {
+    return variant == 3 || variant == 4 ? 23 : variant >= 6 ? 11 : 15;
+}
+constexpr bool batch_variant_takes(int variant, int ipt) {
+    return batch_variant_max_ipt(variant) == 23 ? (ipt == 15 || ipt == 19 || ipt == 23)
+                                                : ((ipt == 7 || ipt == 11 || ipt == 15) &&
+                                                   ipt <= batch_variant_max_ipt(variant));
+}
+// The items per lane a variant is timed with before the per-class search.
+constexpr int batch_variant_start_ipt(int variant) {
+    return batch_variant_max_ipt(variant) == 11 ? 11 : 15;
+}
 int batch_warp_launch(int dtype, int variant, const SpmmLaunch& a, cudaStream_t s);
 // The tuning cache, shared by merbit_plan_tune and merbit_batch_tune: the
 // items per lane of the batched k = 1 kernel for a plan's signature (-1:
-// nothing cached), and the store of a batch tuner's choice.
-int tune_cache_batch_ipt(const merbit_plan_s* p);
-void tune_cache_store_batch_ipt(const merbit_plan_s* p, int ipt);
+// nothing cached) and the variant it was tuned in (*variant, -1 when only a
+// warp-tile SpMV configuration suggested it), and the store of a batch
+// tuner's choice.
+int tune_cache_batch_ipt(const merbit_plan_s* p, int* variant);
+void tune_cache_store_batch_ipt(const merbit_plan_s* p, int variant, int ipt);
 bool spmm_config_exists(int k, int vw, int items);
+// The tile sizes (merge items) the SpMM kernel has for k right-hand sides,
+// into out[4]; returns how many.
+int spmm_tile_candidates(int k, int* out);
 
 }  // namespace merbit
 

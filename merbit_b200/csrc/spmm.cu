@@ -689,6 +689,18 @@ int launch_spmm_dt(int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s
     MERBIT_SPMM_CASE(8, 4, 512)
     MERBIT_SPMM_CASE(16, 4, 512)
     MERBIT_SPMM_CASE(32, 4, 512)
+    // odd segments per lane group (tile = groups x odd length): the groups'
+    // shared-memory reads start in different banks
+    MERBIT_SPMM_CASE(1, 1, 288)
+    MERBIT_SPMM_CASE(1, 1, 480)
+    MERBIT_SPMM_CASE(4, 4, 288)
+    MERBIT_SPMM_CASE(4, 4, 480)
+    MERBIT_SPMM_CASE(8, 4, 272)
+    MERBIT_SPMM_CASE(8, 4, 496)
+    MERBIT_SPMM_CASE(16, 4, 264)
+    MERBIT_SPMM_CASE(16, 4, 504)
+    MERBIT_SPMM_CASE(32, 4, 260)
+    MERBIT_SPMM_CASE(32, 4, 508)
 #undef MERBIT_SPMM_CASE
     return fail(MERBIT_ERR_INVALID, "spmm: no such configuration");
 }
@@ -698,7 +710,26 @@ int launch_spmm_dt(int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s
 bool spmm_config_exists(int k, int vw, int items) {
     if (items == 256) return (k == 1 && vw == 1) || (k >= 2 && k <= 32 && (k & (k - 1)) == 0 && vw <= 4 && vw <= k && (vw & (vw - 1)) == 0 && !(k == 2 && vw == 4));
     if (items == 512) return (k == 1 && vw == 1) || (k >= 4 && k <= 32 && (k & (k - 1)) == 0 && vw == 4);
+    if (k == 1) return vw == 1 && (items == 288 || items == 480);
+    if (vw != 4) return false;
+    switch (k) {
+    case 4: return items == 288 || items == 480;
+    case 8: return items == 272 || items == 496;
+    case 16: return items == 264 || items == 504;
+    case 32: return items == 260 || items == 508;
+    }
     return false;
+}
+
+int spmm_tile_candidates(int k, int* out) {
+    int n = 0;
+    out[n++] = 256;
+    out[n++] = 512;
+    static const int odd[6][2] = {{288, 480}, {0, 0}, {288, 480}, {272, 496}, {264, 504}, {260, 508}};
+    const int row = k == 1 ? 0 : k == 4 ? 2 : k == 8 ? 3 : k == 16 ? 4 : k == 32 ? 5 : 1;
+    for (int j = 0; j < 2; ++j)
+        if (odd[row][j]) out[n++] = odd[row][j];
+    return n;
 }
 
 int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s) {

@@ -276,7 +276,13 @@ constexpr SpmvConfig kCfgF64[] = {
     {3, 256, 8, 1, 0, 1},            {3, 256, 16, 1, 0, 1},
     {3, 256, 2, 1, 0, 0},            {3, 256, 4, 1, 0, 0, 1},
     {3, 256, 2, 1, 0, 0, 1},         {3, 256, 8, 1, 0, 0, 1},
-    {3, 256, 1, 1, 0, 0, 1}};
+    {3, 256, 1, 1, 0, 0, 1},
+    // warp tiles added later (appended, so earlier indices stay): 13 items
+    // per lane (4 CTAs of 8 warps at the 72% carveout in FP64), and tiles
+    // with a row_ptr window for every item (stg = 1: no rows-per-tile cap),
+    // with L1 gathers at a 58% carveout for matrices whose columns repeat
+    {1, 256, 13, 1, kCarveoutL1, 1},  {1, 256, 11, 1, kCarveoutL1Max, 0, 1},
+    {1, 256, 15, 1, kCarveoutL1Max, 0, 1}, {1, 256, 11, 1, kCarveoutL1, 1, 1}};
 constexpr SpmvConfig kCfgF32[] = {
     {1, 256, 15, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1, 1},
     {1, 256, 11, 1, kCarveoutL1, 1}, {1, 128, 15, 1, kCarveoutL1Max, 1},
@@ -290,7 +296,13 @@ constexpr SpmvConfig kCfgF32[] = {
     {3, 256, 8, 1, 0, 1},            {3, 256, 16, 1, 0, 1},
     {3, 256, 2, 1, 0, 0},            {3, 256, 4, 1, 0, 0, 1},
     {3, 256, 2, 1, 0, 0, 1},         {3, 256, 8, 1, 0, 0, 1},
-    {3, 256, 1, 1, 0, 0, 1}};
+    {3, 256, 1, 1, 0, 0, 1},
+    // warp tiles added later (appended, so earlier indices stay): 13 items
+    // per lane (4 CTAs of 8 warps at the 72% carveout in FP64), and tiles
+    // with a row_ptr window for every item (stg = 1: no rows-per-tile cap),
+    // with L1 gathers at a 58% carveout for matrices whose columns repeat
+    {1, 256, 13, 1, kCarveoutL1, 1},  {1, 256, 11, 1, kCarveoutL1Max, 0, 1},
+    {1, 256, 15, 1, kCarveoutL1Max, 0, 1}, {1, 256, 11, 1, kCarveoutL1, 1, 1}};
 
 template <int DT, int BLOCK, int IPT, bool VEC, bool RES>
 int launch_one_k(const SpmvLaunch& a, cudaStream_t s) {
@@ -354,7 +366,8 @@ int spmv_tile_items(const SpmvConfig& c) {
 bool spmv_config_allowed(const SpmvConfig& c, bool vec) { return vec || c.kind == 0 || c.kind == 3; }
 
 int spmv_config_row_cap(const SpmvConfig& c) {
-    return c.kind == 1 ? warp_rp_cap(c.ipt) - 8 : INT_MAX;
+    // warp tiles with stg = 1 stage a row_ptr window for every item of the tile
+    return c.kind == 1 && !c.stg ? warp_rp_cap(c.ipt) - 8 : INT_MAX;
 }
 
 

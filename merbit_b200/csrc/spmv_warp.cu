@@ -67,9 +67,15 @@ struct SpmvSrc {
 
 // CV: the shared-memory carveout the kernel is launched with (it does not
 // change the code; each split gets its own function and function attribute).
-template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG, int CV>
+// FULL: the row_ptr window holds a tile whose every item ends a row (no cap
+// on rows per tile; matrices with runs of empty rows), else warp_rp_cap(IPT).
+template <int DT, int IPT, bool FULL>
+using SpmvWarpSmem = WarpSmem<typename Prec<DT>::V, typename Prec<DT>::P, IPT,
+                              FULL ? 32 * IPT + 16 : warp_rp_cap(IPT)>;
+
+template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG, int CV, bool FULL>
 __global__ void __launch_bounds__(WARPS * 32) spmv_warp_kernel(const SpmvLaunch a) {
-    using T = WarpTile<DT, IPT, CG>;
+    using T = WarpTile<DT, IPT, CG, SpmvWarpSmem<DT, IPT, FULL>>;
     using S = typename T::S;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned s_epoch;
@@ -189,19 +195,19 @@ int launch_coop(K kern, int warps, size_t smem, int carveout, int* grid_cap, con
     return e == cudaSuccess ? (int)MERBIT_OK : cuda_fail(e, name);
 }
 
-template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG, int CV>
+template <int DT, int WARPS, int IPT, int STAGES, bool RES, bool CG, int CV, bool FULL>
 int launch_warp_k(const SpmvLaunch& a, cudaStream_t s) {
-    using S = typename WarpTile<DT, IPT, CG>::S;
+    using S = SpmvWarpSmem<DT, IPT, FULL>;
     static int grid_cap[64] = {};
     if (RES && !a.partials) return fail(MERBIT_ERR_INVALID, "spmv_warp: residual without partials");
-    return launch_coop(spmv_warp_kernel<DT, WARPS, IPT, STAGES, RES, CG, CV>, WARPS,
+    return launch_coop(spmv_warp_kernel<DT, WARPS, IPT, STAGES, RES, CG, CV, FULL>, WARPS,
                        S::bytes * WARPS * STAGES, CV, grid_cap, a, s, "spmv_warp_kernel");
 }
 
-template <int DT, int WARPS, int IPT, int STAGES, bool CG, int CV>
+template <int DT, int WARPS, int IPT, int STAGES, bool CG, int CV, bool FULL = false>
 int launch_warp(const SpmvLaunch& a, cudaStream_t s) {
-    return a.residual ? launch_warp_k<DT, WARPS, IPT, STAGES, true, CG, CV>(a, s)
-                      : launch_warp_k<DT, WARPS, IPT, STAGES, false, CG, CV>(a, s);
+    return a.residual ? launch_warp_k<DT, WARPS, IPT, STAGES, true, CG, CV, FULL>(a, s)
+                      : launch_warp_k<DT, WARPS, IPT, STAGES, false, CG, CV, FULL>(a, s);
 }
 
 // The (warps, items per thread, gather hint, carveout) combinations of the
@@ -211,8 +217,11 @@ int launch_warp_dt(const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s) {
     const int warps = c.block / 32, ipt = c.ipt;
     if (c.stages != 1) return fail(MERBIT_ERR_INVALID, "spmv_warp: no such configuration");
 #define MERBIT_WARP_CASE(W, I, G, C)                                                   \
-    if (warps == W && ipt == I && c.cg == G && c.carveout == C)                        \
+    if (warps == W && ipt == I && c.cg == G && c.carveout == C && !c.stg)              \
         return launch_warp<DT, W, I, 1, G, C>(a, s);
+#define MERBIT_WARP_FULL_CASE(W, I, G, C)                                              \
+    if (warps == W && ipt == I && c.cg == G && c.carveout == C && c.stg)               \
+        return launch_warp<DT, W, I, 1, G, C, true>(a, s);
     MERBIT_WARP_CASE(8, 15, 1, kCarveoutL1)
     MERBIT_WARP_CASE(4, 15, 1, kCarveoutL1)
     MERBIT_WARP_CASE(8, 11, 1, kCarveoutL1)
@@ -223,7 +232,12 @@ int launch_warp_dt(const SpmvConfig& c, const SpmvLaunch& a, cudaStream_t s) {
     MERBIT_WARP_CASE(8, 11, 0, 0)
     MERBIT_WARP_CASE(8, 7, 0, 0)
     MERBIT_WARP_CASE(4, 23, 0, 0)
+    MERBIT_WARP_CASE(8, 13, 1, kCarveoutL1)
+    MERBIT_WARP_FULL_CASE(8, 11, 0, kCarveoutL1Max)
+    MERBIT_WARP_FULL_CASE(8, 15, 0, kCarveoutL1Max)
+    MERBIT_WARP_FULL_CASE(8, 11, 1, kCarveoutL1)
 #undef MERBIT_WARP_CASE
+#undef MERBIT_WARP_FULL_CASE
     return fail(MERBIT_ERR_INVALID, "spmv_warp: no such configuration");
 }
 }  // namespace

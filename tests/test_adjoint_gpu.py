@@ -90,7 +90,10 @@ def test_gradcheck_fp64_finite_differences_fast_mode():
 def test_gradcheck_fp64_finite_differences_full_jacobian(wrt):
     """The full Jacobian of the 2,000-row instance against FP64 central
     differences, one input at a time: d Y / d vals (14,006 x 2,000, k = 1)
-    and d Y / d X (k = 2)."""
+    and d Y / d X (k = 2).  Y is linear in vals and in X, so a central
+    difference has no truncation error at any step; the step 1e-4 keeps its
+    rounding error (about max|Y| * 2^-52 / step, max|Y| ~ 30 on rows of up
+    to 960 entries) below the 1e-9 absolute tolerance."""
     A = _diff_instance()
     rp, col, v = to_cuda(A, "f64")
     k = 1 if wrt == "vals" else 2
@@ -102,7 +105,7 @@ def test_gradcheck_fp64_finite_differences_full_jacobian(wrt):
         fn, inputs = (lambda w: M.matmul(X, vals=w)), (vals,)
     else:
         fn, inputs = (lambda x: M.matmul(x, vals=vals)), (X,)
-    assert torch.autograd.gradcheck(fn, inputs, eps=1e-6, atol=1e-9, rtol=1e-7)
+    assert torch.autograd.gradcheck(fn, inputs, eps=1e-4, atol=1e-9, rtol=1e-7)
 
 
 @pytest.mark.gpu

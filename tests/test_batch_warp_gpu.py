@@ -1,6 +1,6 @@
 """The batched k = 1 warp-tile kernel (merbit_batch_spmm with one right-hand
 side): many uneven matrices in one persistent launch, each with its own
-tile size (7, 11 or 15 items per lane).
+tile size (7, 11, 15, 19 or 23 items per lane).
 
 Each matrix's y must be bitwise the y of the single-matrix warp-tile SpMV
 with the same items per lane (same partition, same order of additions),
@@ -51,15 +51,19 @@ def _build(mats, dtype, beta_y0=None):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
-@pytest.mark.parametrize("ipt", [7, 11, 15, "mixed"])
-def test_batch_k1_matches_single_matrix_warp_kernel(dtype, ipt):
+@pytest.mark.parametrize("variant,ipt", [(0, 7), (0, 11), (1, 15), (2, "mixed"), (3, 19),
+                                         (4, 23), (3, "mixed"), (5, "mixed"), (6, "mixed"),
+                                         (7, 11), (8, "mixed"), (9, "mixed")])
+def test_batch_k1_matches_single_matrix_warp_kernel(dtype, variant, ipt):
     mats = _mats()
     plans, Xs, Ys, xh = _build(mats, dtype)
     batch = mb.Batch(plans, Xs, Ys)
-    ipts = [[7, 11, 15][i % 3] if ipt == "mixed" else ipt for i in range(len(mats))]
+    batch.set_kernel(1, variant)
+    takes = {3: (15, 19, 23), 4: (15, 19, 23)}.get(variant, (7, 11) if variant >= 6 else (7, 11, 15))
+    ipts = [takes[i % len(takes)] if ipt == "mixed" else ipt for i in range(len(mats))]
     for i, p in enumerate(ipts):
         batch.set_matrix_config(i, p)
-    assert batch.info()["kernel"] == 1
+    assert batch.info()["kernel"] == 1 and batch.info()["variant"] == variant
     assert [c[2] for c in batch.matrix_configs()] == ipts
     assert [c[1] for c in batch.matrix_configs()] == [32 * p for p in ipts]
     batch.run()
@@ -78,7 +82,9 @@ def test_batch_k1_matches_single_matrix_warp_kernel(dtype, ipt):
             torch.cuda.synchronize()
             assert torch.equal(ys, Ys[i][:, 0]), (i, A.nrow, A.nnz, ipts[i])
             compared += 1
-    assert compared >= len(mats) // 2
+    # the single-matrix table has warp tiles of 7, 11, 15 and 23 items per lane
+    if set(ipts) <= {7, 11, 15, 23}:
+        assert compared >= len(mats) // 2
     batch.close()
 
 
@@ -115,7 +121,7 @@ def test_batch_k1_graph_replay_alpha_beta_and_tuning():
     cfgs = batch.matrix_configs()
     assert len(cfgs) == len(mats)
     if info["kernel"] == 1:
-        assert all(c[2] in (7, 11, 15) and c[1] == 32 * c[2] for c in cfgs)
+        assert all(c[2] in (7, 11, 15, 19, 23) and c[1] == 32 * c[2] for c in cfgs)
         # a new batch of the same matrices starts from the cached choices
         b2 = mb.Batch(plans, Xs, Ys)
         assert b2.info()["kernel"] == 1
@@ -133,3 +139,39 @@ def test_batch_matrix_config_arguments_need_no_gpu():
     L = mb.lib()
     assert L.merbit_batch_set_matrix_config(None, 0, 11, None) == 1
     assert L.merbit_batch_get_matrix_config(None, 0, None, None, None) == 1
+    assert L.merbit_batch_set_kernel(None, 1, 0, None) == 1
+
+
+@pytest.mark.gpu
+def test_batch_kernel_selection_and_refusals():
+    """Every SpMM tile size of each k, and the warp-tile variants at k = 1,
+    give the oracle's answer; items per lane a variant does not take are
+    refused, as is the warp-tile kernel at k > 1."""
+    mats = _mats()[:6]
+    for k in (1, 4, 8, 16, 32):
+        plans, Xs, Ys, xh = [], [], [], []
+        for i, A in enumerate(mats):
+            rp, col, v = to_cuda(A, "f32")
+            plans.append(mb.Plan(rp, col, v, ncol=A.ncol))
+            x = synth.uniform(70 + i, A.ncol * k).astype(np.float32).reshape(A.ncol, k)
+            xh.append(x)
+            Xs.append(torch.from_numpy(x).cuda())
+            Ys.append(torch.empty(A.nrow, k, dtype=torch.float32, device="cuda"))
+        batch = mb.Batch(plans, Xs, Ys)
+        odd = {1: (288, 480), 4: (288, 480), 8: (272, 496), 16: (264, 504), 32: (260, 508)}[k]
+        choices = [(0, t) for t in (256, 512) + odd] + ([(1, v) for v in range(10)] if k == 1 else [])
+        for kern, opt in choices:
+            batch.set_kernel(kern, opt)
+            batch.run()
+            torch.cuda.synchronize()
+            for i, A in enumerate(mats):
+                yo, ya = O.spmm(A.row_ptr, A.col, A.vals.astype(np.float32), xh[i], k=k)
+                assert O.rel_error(Ys[i].cpu().numpy(), yo, ya)[0] <= TOL["f32"], (k, kern, opt, i)
+        if k == 1:
+            batch.set_kernel(1, 0)
+            with pytest.raises(mb.MerbitError):
+                batch.set_matrix_config(0, 23)
+        else:
+            with pytest.raises(mb.MerbitError):
+                batch.set_kernel(1, 0)
+        batch.close()
