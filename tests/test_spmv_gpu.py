@@ -300,3 +300,33 @@ def test_graph_replay_every_config(dtype, workload):
                 assert e <= TOL[dtype], (idx, kind, rep, j, e)
         del g
         plan.check()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
+def test_warp_configs_with_equal_tiles_agree_bitwise(dtype):
+    """Warp-tile configurations that differ only in carveout, gather hint,
+    row_ptr window or walk (staged products or the register walk) share the
+    partition and the order of every addition: their y are the same bits."""
+    mats = [A for _, A in edge_cases()] + [synth.rmat(3000, 12, seed=5)]
+    for A in mats:
+        if A.nrow == 0:
+            continue
+        x = _x(A, dtype)
+        rp, col, v = to_cuda(A, dtype)
+        plan = mb.Plan(rp, col, v, ncol=A.ncol)
+        xd = torch.from_numpy(x).cuda()
+        by_ipt = {}
+        for idx, kind, block, ipt in plan.configs():
+            if kind == 1:
+                by_ipt.setdefault(ipt, []).append(idx)
+        for ipt, idxs in by_ipt.items():
+            ys = []
+            for idx in idxs:
+                plan.set_config(idx)
+                ys.append(plan.spmv(xd).clone())
+            torch.cuda.synchronize()
+            plan.check()
+            for idx, y in zip(idxs[1:], ys[1:]):
+                assert torch.equal(y, ys[0]), (A.name, ipt, idxs[0], idx)
+        plan.close()
