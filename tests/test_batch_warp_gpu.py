@@ -175,3 +175,30 @@ def test_batch_kernel_selection_and_refusals():
             with pytest.raises(mb.MerbitError):
                 batch.set_kernel(1, 0)
         batch.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", [0, 6])
+def test_batch_k1_with_empty_members(variant):
+    """Members with no rows, with rows but no nonzeros, and with a single
+    giant row sit between ordinary ones; warps cross them on the way."""
+    mats = [csr_from_lengths([], ncol=5, seed=1),
+            synth.rmat(2000, 10, seed=3),
+            csr_from_lengths([0] * 700, ncol=50, seed=2),
+            csr_from_lengths([], ncol=1, seed=1),
+            csr_from_lengths([90_000], ncol=120_000, seed=4),
+            synth.rmat(5000, 6, seed=6)]
+    plans, Xs, Ys, xh = _build(mats, "f64")
+    batch = mb.Batch(plans, Xs, Ys)
+    batch.set_kernel(1, variant)
+    for rep in range(2):
+        batch.run()
+        torch.cuda.synchronize()
+        for i, A in enumerate(mats):
+            if A.nrow == 0:
+                continue
+            y = Ys[i][:, 0].cpu().numpy()
+            yo, ya = O.spmm(A.row_ptr, A.col, A.vals, xh[i])
+            assert O.rel_error(y, yo, ya)[0] <= TOL["f64"], (rep, i)
+            assert np.all(y[np.diff(A.row_ptr) == 0] == 0)
+    batch.close()
