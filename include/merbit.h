@@ -270,12 +270,10 @@ int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info);
 int merbit_batch_get_matrix_config(merbit_batch batch, int32_t index, int32_t* kernel,
                                    int32_t* tile_items, int32_t* items_per_thread);
 /* Selects the batch's kernel by hand (as merbit_plan_set_config does for a
- * plan): kernel 0, the SpMM kernel with `option` = tile items + 100000 x
- * vector width (0: the widest legal width up to 4).  Tiles are 256 or 512
- * merge items, or an odd number of items per lane group: at width 4,
- * 288/480 for k = 1 or 4, 272/496 for k = 8, 264/504 for k = 16, 260/508
- * for k = 32; at width 8 (k = 8, 16, 32), 288/480, 272/496, 264/504.
- * Kernel 1, the warp-tile kernel (k = 1,
+ * plan): kernel 0, the SpMM kernel with `option` merge items per tile (256
+ * or 512; with vector width 4 also tiles of an odd number of items per lane
+ * group: 288/480 for k = 1 or 4, 272/496 for k = 8, 264/504 for k = 16,
+ * 260/508 for k = 32; widest legal vector width); kernel 1, the warp-tile kernel (k = 1,
  * 16-byte aligned arrays) in variant `option` (0-9, see merbit_batch_info).
  * Synchronizes. */
 int merbit_batch_set_kernel(merbit_batch batch, int32_t kernel, int32_t option, void* stream);

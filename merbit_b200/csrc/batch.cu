@@ -35,9 +35,6 @@ int alloc_spmm_slots(SpmmSlots* s, long long nslots, cudaStream_t st) {
 namespace {
 
 constexpr int kDefaultItems = 256;
-// Widest vector per lane the single-matrix SpMM uses (the batch tuner
-// times every width).
-constexpr int kSingleMaxVw = 4;
 constexpr int kBatchDefaultIpt = 11;
 constexpr int kBatchDefaultVariant = 6;
 
@@ -47,7 +44,7 @@ bool pow2(int k) { return k > 0 && (k & (k - 1)) == 0; }
 // pointers allow for k columns of a type of `esz` bytes.
 int pick_vw(int k, long long ldx, const void* x, const void* y, long long ldy, int esz,
             int items) {
-    for (int vw = 8; vw >= 1; vw >>= 1) {
+    for (int vw = 4; vw >= 1; vw >>= 1) {
         if (vw > k || !spmm_config_exists(k, vw, items)) continue;
         if (vw == 1) return 1;
         const size_t a = (size_t)vw * esz;  // vector load size
@@ -93,12 +90,19 @@ int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long 
             while (vw > 1 && (dv_ldx % vw != 0 || (uintptr_t)dv_x % ((size_t)vw * esz) != 0)) vw >>= 1;
         return vw;
     };
-    // the 512-item tiles (vector width 4) measured faster for k >= 4 on the
-    // power-law and banded matrices; other shapes keep 256
+    // at vector width 4 (k >= 4) the larger tiles measured faster on the
+    // power-law and banded matrices, and among them the one of an odd length
+    // per lane group (480, 496, 504, 508 items at k = 4, 8, 16, 32: no bank
+    // conflicts between the groups' segments; Zipf-1M at k = 16: 0.524 ms
+    // against 0.570 at 512); other shapes keep 256
     int items = kDefaultItems;
-    if (kk >= 4 && width(512) >= 4) items = 512;
-    int vw = width(items);
-    if (vw > kSingleMaxVw) vw = kSingleMaxVw;
+    if (kk >= 4 && width(512) == 4) {
+        items = 512;
+        int cand[4];
+        const int n = spmm_tile_candidates(kk, cand);
+        if (n == 4 && width(cand[3]) == 4) items = cand[3];
+    }
+    const int vw = width(items);
     if (!spmm_config_exists(kk, vw, items)) return MERBIT_ERR_UNSUPPORTED;
     const Partition* part = nullptr;
     int st = plan_partition(p, items, &part, s);
@@ -141,7 +145,6 @@ struct merbit_batch_s {
     // 16-byte aligned arrays): the warp-tile kernel with variant `variant`
     // and ipt[i] items per lane for matrix i
     int kernel = 0, variant = 0;
-    int vw_cap = 4;  // widest vector per lane the SpMM kernel may take
     std::vector<int> ipt;
     bool all_vec = true;
     int device = 0;
@@ -193,11 +196,11 @@ int batch_build(merbit_batch_s* b, int items, cudaStream_t s) {
         h[i] = make_desc(b->plans[i], part, b->x[i], b->ldx[i], b->y[i], b->ldy[i], (int)tot);
         tot += part->num_tiles;
     }
-    int vw = b->vw_cap;
+    int vw = 4;
     const int esz = (int)xy_size(b->dtype);
     for (int i = 0; i < b->count; ++i)
         vw = std::min(vw, pick_vw(b->k, b->ldx[i], b->x[i], b->y[i], b->ldy[i], esz, items));
-    while (vw > 1 && !spmm_config_exists(b->k, vw, items)) vw >>= 1;
+    if (!spmm_config_exists(b->k, vw, items)) vw = 1;
     int st = batch_upload(b, h, tot, s);
     if (st != MERBIT_OK) return st;
     b->kernel = 0;
@@ -412,28 +415,25 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
     int best_kernel = batch->kernel, best_items = batch->items, best_vw = batch->vw;
     int best_variant = batch->variant;
     float best = 1e30f;
-    // the SpMM kernel: every vector width the operands allow, every tile
-    // size of that width
-    const int vw_cap0 = batch->vw_cap;
-    for (int cap = 8; cap >= 1 && st == MERBIT_OK; cap >>= 1) {
-        int items_c[4];
-        const int nitems = spmm_tile_candidates(batch->k, cap, items_c);
-        for (int ii = 0; ii < nitems && st == MERBIT_OK; ++ii) {
-            batch->vw_cap = cap;
-            st = batch_build(batch, items_c[ii], s);
-            if (st != MERBIT_OK) break;
-            if (batch->vw != cap) continue;  // the operands do not allow this width
+    int items_c[4];
+    const int nitems = spmm_tile_candidates(batch->k, items_c);
+    for (int ii = 0; ii < nitems && st == MERBIT_OK; ++ii) {
+        st = batch_build(batch, items_c[ii], s);
+        if (st != MERBIT_OK) break;
+        const int vmax = batch->vw;
+        for (int vw = vmax; vw >= 1 && st == MERBIT_OK; vw >>= 1) {
+            if (!spmm_config_exists(batch->k, vw, items_c[ii])) continue;
+            batch->vw = vw;
             float ms = 0.f;
             st = time_batch(batch, s, e0, e1, 3, &ms);
             if (st == MERBIT_OK && ms < best) {
                 best = ms;
                 best_kernel = 0;
                 best_items = items_c[ii];
-                best_vw = cap;
+                best_vw = vw;
             }
         }
     }
-    batch->vw_cap = vw_cap0;
     // the warp-tile kernel's variants, every matrix at the variant's
     // starting items per lane
     const bool warp_ok = batch->k == 1 && batch->all_vec;
@@ -487,28 +487,23 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
     cudaEventDestroy(e1);
     if (st != MERBIT_OK) return st;
     if (best_kernel == 1) return batch_build_warp(batch, best_variant, s);
-    batch->vw_cap = best_vw;
-    return batch_build(batch, best_items, s);
+    st = batch_build(batch, best_items, s);
+    if (st != MERBIT_OK) return st;
+    batch->vw = best_vw;
+    return MERBIT_OK;
 }
 
 int merbit_batch_set_kernel(merbit_batch batch, int32_t kernel, int32_t option, void* stream) {
     if (!batch) return fail(MERBIT_ERR_INVALID, "batch_set_kernel: batch is null");
     cudaStream_t s = (cudaStream_t)stream;
     if (kernel == 0) {
-        // option = tile items, or tile items + 100000 * vector width
-        const int items = option % 100000, vw = option / 100000;
-        if (vw != 0 && vw != 1 && vw != 2 && vw != 4 && vw != 8)
-            return fail(MERBIT_ERR_INVALID, "batch_set_kernel: vector width is 1, 2, 4 or 8");
+        int cand[4];
+        const int n = spmm_tile_candidates(batch->k, cand);
         bool known = false;
-        for (int w = 8; w >= 1 && !known; w >>= 1)
-            known = (vw == 0 || vw == w) && spmm_config_exists(batch->k, w, items);
+        for (int i = 0; i < n; ++i) known = known || cand[i] == option;
         if (!known)
             return fail(MERBIT_ERR_INVALID, "batch_set_kernel: no SpMM tile of that size for this k");
-        batch->vw_cap = vw ? vw : 4;
-        const int st = batch_build(batch, items, s);
-        if (st == MERBIT_OK && vw && batch->vw != vw)
-            return fail(MERBIT_ERR_INVALID, "batch_set_kernel: the operands do not allow that vector width");
-        return st;
+        return batch_build(batch, option, s);
     }
     if (kernel == 1) {
         if (batch->k != 1 || !batch->all_vec)

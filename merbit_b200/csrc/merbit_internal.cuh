@@ -599,9 +599,9 @@ int batch_warp_launch(int dtype, int variant, const SpmmLaunch& a, cudaStream_t 
 int tune_cache_batch_ipt(const merbit_plan_s* p, int* variant);
 void tune_cache_store_batch_ipt(const merbit_plan_s* p, int variant, int ipt);
 bool spmm_config_exists(int k, int vw, int items);
-// The tile sizes (merge items) the SpMM kernel has for k right-hand sides
-// at vw values per lane, into out[4]; returns how many.
-int spmm_tile_candidates(int k, int vw, int* out);
+// The tile sizes (merge items) the SpMM kernel has for k right-hand sides,
+// into out[4]; returns how many.
+int spmm_tile_candidates(int k, int* out);
 
 }  // namespace merbit
 

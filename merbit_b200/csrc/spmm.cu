@@ -40,18 +40,7 @@ constexpr size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
 
 template <int VW>
 __device__ __forceinline__ void ld_vec(const float* p, float (&o)[VW]) {
-    if (VW == 8) {
-        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
-        const float4 u = __ldg(reinterpret_cast<const float4*>(p) + 1);
-        o[0] = t.x;
-        o[1] = t.y;
-        o[2] = t.z;
-        o[3] = t.w;
-        o[4] = u.x;
-        o[5] = u.y;
-        o[6] = u.z;
-        o[7] = u.w;
-    } else if (VW == 4) {
+    if (VW == 4) {
         const float4 t = __ldg(reinterpret_cast<const float4*>(p));
         o[0] = t.x;
         o[1] = t.y;
@@ -217,10 +206,9 @@ struct SpmmTile {
     static constexpr int SEG = ITEMS / G;   // merge items per group
     // nonzeros gathered ahead: 8 values per lane; at k = 1 (one lane per
     // group, latency-bound) 4, which measured 12% faster on the 128-matrix
-    // R-MAT batch (2.25 -> 1.98 ms; 16 ahead: 2.55 ms); at 8 values per lane
-    // 2 (pairs of nonzeros enter the compensated sums together).  The chunk
-    // size does not change the order of the additions.
-    static constexpr int CH = K == 1 ? 4 : VW >= 8 ? 2 : 8 / VW;
+    // R-MAT batch (2.25 -> 1.98 ms; 16 ahead: 2.55 ms).  The chunk size does
+    // not change the order of the additions.
+    static constexpr int CH = K == 1 ? 4 : 8 / VW;
     static constexpr int CAP = ITEMS + 32;
     static constexpr int RPC = ITEMS + 16;  // row_ptr window (any rows per tile)
     static constexpr size_t rp_bytes = a16((size_t)RPC * 4);
@@ -713,72 +701,34 @@ int launch_spmm_dt(int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s
     MERBIT_SPMM_CASE(16, 4, 504)
     MERBIT_SPMM_CASE(32, 4, 260)
     MERBIT_SPMM_CASE(32, 4, 508)
-    // 8 values per lane: half the lanes per group, so the walk's control
-    // code runs once per 8 columns
-    MERBIT_SPMM_CASE(8, 8, 256)
-    MERBIT_SPMM_CASE(8, 8, 512)
-    MERBIT_SPMM_CASE(8, 8, 288)
-    MERBIT_SPMM_CASE(8, 8, 480)
-    MERBIT_SPMM_CASE(16, 8, 256)
-    MERBIT_SPMM_CASE(16, 8, 512)
-    MERBIT_SPMM_CASE(16, 8, 272)
-    MERBIT_SPMM_CASE(16, 8, 496)
-    MERBIT_SPMM_CASE(32, 8, 256)
-    MERBIT_SPMM_CASE(32, 8, 512)
-    MERBIT_SPMM_CASE(32, 8, 264)
-    MERBIT_SPMM_CASE(32, 8, 504)
 #undef MERBIT_SPMM_CASE
     return fail(MERBIT_ERR_INVALID, "spmm: no such configuration");
 }
 
 }  // namespace
 
-// Odd-segment tiles (groups x odd length) of (k, vw): lanes per group
-// LPG = k / vw, groups G = 32 / LPG.
-static int odd_tiles(int k, int vw, int* out) {
-    if (vw == 8) {
-        static const int t8[3][2] = {{288, 480}, {272, 496}, {264, 504}};  // k = 8, 16, 32
-        const int r = k == 8 ? 0 : k == 16 ? 1 : k == 32 ? 2 : -1;
-        if (r < 0) return 0;
-        out[0] = t8[r][0];
-        out[1] = t8[r][1];
-        return 2;
-    }
-    if (k == 1 && vw == 1) {
-        out[0] = 288;
-        out[1] = 480;
-        return 2;
-    }
-    if (vw != 4) return 0;
-    switch (k) {
-    case 4: out[0] = 288; out[1] = 480; return 2;
-    case 8: out[0] = 272; out[1] = 496; return 2;
-    case 16: out[0] = 264; out[1] = 504; return 2;
-    case 32: out[0] = 260; out[1] = 508; return 2;
-    }
-    return 0;
-}
-
 bool spmm_config_exists(int k, int vw, int items) {
-    if (vw == 8) {
-        if (k != 8 && k != 16 && k != 32) return false;
-        if (items == 256 || items == 512) return true;
-    } else {
-        if (items == 256) return (k == 1 && vw == 1) || (k >= 2 && k <= 32 && (k & (k - 1)) == 0 && vw <= 4 && vw <= k && (vw & (vw - 1)) == 0 && !(k == 2 && vw == 4));
-        if (items == 512) return (k == 1 && vw == 1) || (k >= 4 && k <= 32 && (k & (k - 1)) == 0 && vw == 4);
+    if (items == 256) return (k == 1 && vw == 1) || (k >= 2 && k <= 32 && (k & (k - 1)) == 0 && vw <= 4 && vw <= k && (vw & (vw - 1)) == 0 && !(k == 2 && vw == 4));
+    if (items == 512) return (k == 1 && vw == 1) || (k >= 4 && k <= 32 && (k & (k - 1)) == 0 && vw == 4);
+    if (k == 1) return vw == 1 && (items == 288 || items == 480);
+    if (vw != 4) return false;
+    switch (k) {
+    case 4: return items == 288 || items == 480;
+    case 8: return items == 272 || items == 496;
+    case 16: return items == 264 || items == 504;
+    case 32: return items == 260 || items == 508;
     }
-    int odd[2];
-    const int n = odd_tiles(k, vw, odd);
-    for (int i = 0; i < n; ++i)
-        if (odd[i] == items) return true;
     return false;
 }
 
-int spmm_tile_candidates(int k, int vw, int* out) {
+int spmm_tile_candidates(int k, int* out) {
     int n = 0;
-    for (int items : {256, 512})
-        if (spmm_config_exists(k, vw, items)) out[n++] = items;
-    n += odd_tiles(k, vw, out + n);
+    out[n++] = 256;
+    out[n++] = 512;
+    static const int odd[6][2] = {{288, 480}, {0, 0}, {288, 480}, {272, 496}, {264, 504}, {260, 508}};
+    const int row = k == 1 ? 0 : k == 4 ? 2 : k == 8 ? 3 : k == 16 ? 4 : k == 32 ? 5 : 1;
+    for (int j = 0; j < 2; ++j)
+        if (odd[row][j]) out[n++] = odd[row][j];
     return n;
 }
 
