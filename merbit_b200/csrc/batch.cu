@@ -98,9 +98,8 @@ int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long 
     int items = kDefaultItems;
     if (kk >= 4 && width(512) == 4) {
         items = 512;
-        int cand[4];
-        const int n = spmm_tile_candidates(kk, cand);
-        if (n == 4 && width(cand[3]) == 4) items = cand[3];
+        const int odd = spmm_odd_tile(kk);
+        if (odd && width(odd) == 4) items = odd;
     }
     const int vw = width(items);
     if (!spmm_config_exists(kk, vw, items)) return MERBIT_ERR_UNSUPPORTED;
@@ -415,7 +414,7 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
     int best_kernel = batch->kernel, best_items = batch->items, best_vw = batch->vw;
     int best_variant = batch->variant;
     float best = 1e30f;
-    int items_c[4];
+    int items_c[8];
     const int nitems = spmm_tile_candidates(batch->k, items_c);
     for (int ii = 0; ii < nitems && st == MERBIT_OK; ++ii) {
         st = batch_build(batch, items_c[ii], s);
@@ -497,7 +496,7 @@ int merbit_batch_set_kernel(merbit_batch batch, int32_t kernel, int32_t option, 
     if (!batch) return fail(MERBIT_ERR_INVALID, "batch_set_kernel: batch is null");
     cudaStream_t s = (cudaStream_t)stream;
     if (kernel == 0) {
-        int cand[4];
+        int cand[8];
         const int n = spmm_tile_candidates(batch->k, cand);
         bool known = false;
         for (int i = 0; i < n; ++i) known = known || cand[i] == option;

@@ -600,8 +600,10 @@ int tune_cache_batch_ipt(const merbit_plan_s* p, int* variant);
 void tune_cache_store_batch_ipt(const merbit_plan_s* p, int variant, int ipt);
 bool spmm_config_exists(int k, int vw, int items);
 // The tile sizes (merge items) the SpMM kernel has for k right-hand sides,
-// into out[4]; returns how many.
+// into out[8]; returns how many.  spmm_odd_tile: the larger tile of an odd
+// length per lane group at vector width 4 (0 if k has none).
 int spmm_tile_candidates(int k, int* out);
+int spmm_odd_tile(int k);
 
 }  // namespace merbit
 

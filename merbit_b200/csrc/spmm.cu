@@ -101,6 +101,11 @@ struct AccRow {
         add(a0, x0);
         add(a1, x1);
     }
+    // products formed beforehand (one per column)
+    __device__ __forceinline__ void add_p(const P (&p)[VW]) {
+#pragma unroll
+        for (int v = 0; v < VW; ++v) a[v].add(p[v]);
+    }
 };
 
 // TwoSum accumulators of an even number of columns, two columns per packed
@@ -162,6 +167,10 @@ struct AccRow<AccTwoSum, VW, float, float> {
             sum(h, f2_fma(b1, f2_pack(x1[2 * h], x1[2 * h + 1]), p0));
         }
     }
+    __device__ __forceinline__ void add_p(const float (&p)[VW]) {
+#pragma unroll
+        for (int h = 0; h < VW / 2; ++h) sum(h, f2_pack(p[2 * h], p[2 * h + 1]));
+    }
     // TwoSum of p into (s[h], c[h])
     __device__ __forceinline__ void sum(int h, unsigned long long p) {
         const unsigned long long t = f2_add(s[h], p);
@@ -189,6 +198,7 @@ struct AccRow<AccTwoSum, 1, float, float> {
         add(a0, x0);
         add(a1, x1);
     }
+    __device__ __forceinline__ void add_p(const float (&p)[1]) { a.add(p[0]); }
 };
 
 // DV: also form dL/dval for each nonzero (SpmmLaunch::dv_*), from the x row
@@ -209,6 +219,13 @@ struct SpmmTile {
     // R-MAT batch (2.25 -> 1.98 ms; 16 ahead: 2.55 ms).  The chunk size does
     // not change the order of the additions.
     static constexpr int CH = K == 1 ? 4 : 8 / VW;
+    // Staged products (one lane per group, tiles of 224 or 352 items, no
+    // fused dval): the warp gathers the X rows of all the tile's nonzeros
+    // lane-contiguously, every gather in flight at once, and stores the
+    // products in shared memory; each lane then walks its segment from
+    // there.  The chunked walk instead keeps only CH nonzeros ahead per lane.
+    static constexpr bool STAGEP = K == 2 && VW == 2 && (ITEMS == 224 || ITEMS == 352) && !DV;
+    static constexpr int NJ = ITEMS / 32;  // staged products per lane
     static constexpr int CAP = ITEMS + 32;
     static constexpr int RPC = ITEMS + 16;  // row_ptr window (any rows per tile)
     static constexpr size_t rp_bytes = a16((size_t)RPC * 4);
@@ -217,7 +234,9 @@ struct SpmmTile {
     // DV: the tile's slice of the transpose permutation, staged like col
     static constexpr size_t perm_bytes = DV ? a16((size_t)CAP * 4) : 0;
     static constexpr size_t perm_offset = rp_bytes + col_bytes + val_bytes;
-    static constexpr size_t bar_offset = perm_offset + perm_bytes;
+    static constexpr size_t prod_bytes = STAGEP ? a16((size_t)ITEMS * VW * sizeof(P)) : 0;
+    static constexpr size_t prod_offset = perm_offset + perm_bytes;
+    static constexpr size_t bar_offset = prod_offset + prod_bytes;
     static constexpr size_t bytes = bar_offset + 16;
     static constexpr int GV = 16 / (int)sizeof(V);
     static_assert(LPG >= 1 && LPG <= 32 && 32 % LPG == 0, "K/VW must divide 32");
@@ -422,13 +441,47 @@ struct SpmmTile {
                 }
             }
         };
-        if (lx < lx_end) load_chunk(lx, xa, va);
-        for (int c = lx; c < lx_end; c += 2 * CH) {
-            if (c + CH < lx_end) load_chunk(c + CH, xb, vb);
-            consume(c, xa, va);
-            if (c + CH >= lx_end) break;
-            if (c + 2 * CH < lx_end) load_chunk(c + 2 * CH, xa, va);
-            consume(c + CH, xb, vb);
+        if constexpr (STAGEP) {
+            // products of nonzero i (relative to the tile) at s_prod[i * VW]
+            P* s_prod = reinterpret_cast<P*>(ws + prod_offset);
+            {
+                int cidx[NJ];
+#pragma unroll
+                for (int j = 0; j < NJ; ++j) {
+                    const int i = lane + 32 * j;
+                    cidx[j] = i < nz ? s_col[col_o + i] : 0;
+                }
+                X xr[NJ][VW];
+#pragma unroll
+                for (int j = 0; j < NJ; ++j)
+                    if (lane + 32 * j < nz) ld_vec<VW>(xm + (size_t)cidx[j] * d.ldx, xr[j]);
+#pragma unroll
+                for (int j = 0; j < NJ; ++j) {
+                    const int i = lane + 32 * j;
+                    if (i < nz) {
+                        const P av = to_p(s_val[val_o + i]);
+#pragma unroll
+                        for (int v = 0; v < VW; ++v) s_prod[(size_t)i * VW + v] = av * (P)xr[j][v];
+                    }
+                }
+            }
+            __syncwarp();
+            for (int e = lx; e < lx_end; ++e) {
+                end_rows(e);
+                P pv[VW];
+#pragma unroll
+                for (int v = 0; v < VW; ++v) pv[v] = s_prod[(size_t)e * VW + v];
+                acc.add_p(pv);
+            }
+        } else {
+            if (lx < lx_end) load_chunk(lx, xa, va);
+            for (int c = lx; c < lx_end; c += 2 * CH) {
+                if (c + CH < lx_end) load_chunk(c + CH, xb, vb);
+                consume(c, xa, va);
+                if (c + CH >= lx_end) break;
+                if (c + 2 * CH < lx_end) load_chunk(c + 2 * CH, xa, va);
+                consume(c + CH, xb, vb);
+            }
         }
         while (ly < ly_end) {
             emit(ly);
@@ -701,6 +754,12 @@ int launch_spmm_dt(int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s
     MERBIT_SPMM_CASE(16, 4, 504)
     MERBIT_SPMM_CASE(32, 4, 260)
     MERBIT_SPMM_CASE(32, 4, 508)
+    // k = 2, one lane per group with staged products (SpmmTile::STAGEP):
+    // 2.12 ms against 2.84 for the 128-matrix R-MAT batch; at k = 4 the
+    // product slice and registers cost more warps than it saves (3.12 ms
+    // against 2.39), so k = 4 has no such tile
+    MERBIT_SPMM_CASE(2, 2, 224)
+    MERBIT_SPMM_CASE(2, 2, 352)
 #undef MERBIT_SPMM_CASE
     return fail(MERBIT_ERR_INVALID, "spmm: no such configuration");
 }
@@ -710,6 +769,7 @@ int launch_spmm_dt(int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s
 bool spmm_config_exists(int k, int vw, int items) {
     if (items == 256) return (k == 1 && vw == 1) || (k >= 2 && k <= 32 && (k & (k - 1)) == 0 && vw <= 4 && vw <= k && (vw & (vw - 1)) == 0 && !(k == 2 && vw == 4));
     if (items == 512) return (k == 1 && vw == 1) || (k >= 4 && k <= 32 && (k & (k - 1)) == 0 && vw == 4);
+    if (items == 224 || items == 352) return k == 2 && vw == 2;
     if (k == 1) return vw == 1 && (items == 288 || items == 480);
     if (vw != 4) return false;
     switch (k) {
@@ -729,7 +789,21 @@ int spmm_tile_candidates(int k, int* out) {
     const int row = k == 1 ? 0 : k == 4 ? 2 : k == 8 ? 3 : k == 16 ? 4 : k == 32 ? 5 : 1;
     for (int j = 0; j < 2; ++j)
         if (odd[row][j]) out[n++] = odd[row][j];
+    if (k == 2) {  // staged products
+        out[n++] = 224;
+        out[n++] = 352;
+    }
     return n;
+}
+
+int spmm_odd_tile(int k) {
+    switch (k) {
+    case 4: return 480;
+    case 8: return 496;
+    case 16: return 504;
+    case 32: return 508;
+    }
+    return 0;
 }
 
 int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s) {

@@ -148,7 +148,7 @@ def test_batch_kernel_selection_and_refusals():
     give the oracle's answer; items per lane a variant does not take are
     refused, as is the warp-tile kernel at k > 1."""
     mats = _mats()[:6]
-    for k in (1, 4, 8, 16, 32):
+    for k in (1, 2, 4, 8, 16, 32):
         plans, Xs, Ys, xh = [], [], [], []
         for i, A in enumerate(mats):
             rp, col, v = to_cuda(A, "f32")
@@ -158,8 +158,10 @@ def test_batch_kernel_selection_and_refusals():
             Xs.append(torch.from_numpy(x).cuda())
             Ys.append(torch.empty(A.nrow, k, dtype=torch.float32, device="cuda"))
         batch = mb.Batch(plans, Xs, Ys)
-        odd = {1: (288, 480), 4: (288, 480), 8: (272, 496), 16: (264, 504), 32: (260, 508)}[k]
-        choices = [(0, t) for t in (256, 512) + odd] + ([(1, v) for v in range(10)] if k == 1 else [])
+        odd = {1: (288, 480), 2: (224, 352), 4: (288, 480), 8: (272, 496), 16: (264, 504),
+               32: (260, 508)}[k]
+        base = (256,) if k == 2 else (256, 512)
+        choices = [(0, t) for t in base + odd] + ([(1, v) for v in range(10)] if k == 1 else [])
         for kern, opt in choices:
             batch.set_kernel(kern, opt)
             batch.run()
