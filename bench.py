@@ -369,6 +369,29 @@ def component_error(y, y_ref, y_abs) -> dict:
     return {"max": float(e.max()), "median": float(np.median(e))}
 
 
+def l2_flushed_ms(A, rp, col, vals64, x64, dev, stream, reps: int = 20) -> float:
+    """Mean ms of one tuned FP64 SpMV launched after writing a 256 MB buffer
+    (larger than L2), each launch timed on its own with CUDA events."""
+    import torch
+
+    import merbit_b200 as mb
+
+    plan = mb.Plan(rp, col, vals64, ncol=A.ncol)
+    plan.tune(x64)
+    y = torch.empty(A.nrow, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(reps)]
+    for a, b in evs:
+        flush.fill_(1)
+        a.record(stream)
+        plan.spmv(x64, y)
+        b.record(stream)
+    torch.cuda.synchronize(dev)
+    plan.close()
+    return statistics.mean(a.elapsed_time(b) for a, b in evs)
+
+
 def spmv_form(A, dtype: str, rp, col, vals64, x64, steps: int, dev, stream, peak: float,
               workload: str) -> dict:
     """One tuned SpMV of A with values stored as `dtype` (x FP64 for FP64
@@ -604,6 +627,18 @@ def secondary_forms(args, A_zipf, rp, col, vals64, x64, dev, stream, peak,
     zf = {d: spmv_form(A_zipf, d, rp, col, vals64, x64, steps, dev, stream, peak, "zipf_2m")
           for d in ("f32", "bf16")}
     forms["zipf_2m"] = zf
+    # 5-point Laplacian 256^2, FP64 (L2-resident: 5.2 MB): back to back from
+    # a graph, and one launch at a time with L2 flushed before each
+    Lp = synth.workload("laplace2d_256")
+    lrp = torch.from_numpy(Lp.row_ptr).to(dev)
+    lcol = torch.from_numpy(Lp.col).to(dev)
+    lv = torch.from_numpy(Lp.vals).to(dev)
+    lx = torch.from_numpy(synth.workload_x("laplace2d_256", Lp.ncol)).to(dev)
+    lap = spmv_form(Lp, "f64", lrp, lcol, lv, lx, steps, dev, stream, peak, "laplace2d_256")
+    lap["l2"] = "L2-resident between back-to-back launches (ms, gbs); ms_l2_flushed flushes L2"
+    lap["ms_l2_flushed"] = round(l2_flushed_ms(Lp, lrp, lcol, lv, lx, dev, stream), 5)
+    forms["laplace2d_256"] = {"nrow": Lp.nrow, "nnz": Lp.nnz, "f64": lap}
+    del lrp, lcol, lv, lx, Lp
     # 27-point stencil 160^3 in FP64, FP32 and BF16
     S = synth.workload("stencil27_160")
     srp = torch.from_numpy(S.row_ptr).to(dev)
