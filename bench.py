@@ -392,8 +392,18 @@ def l2_flushed_ms(A, rp, col, vals64, x64, dev, stream, reps: int = 20) -> float
     return statistics.mean(a.elapsed_time(b) for a, b in evs)
 
 
+def cpu_fp64_error(A, vals_stored, x_stored, y_gpu) -> dict:
+    """Component-wise error of y_gpu against the FP64 CPU SpMV (the OpenMP
+    restatement of the CPU baseline, oracle/) on the inputs as stored."""
+    from oracle import oracle as O
+
+    ys, _ = O.spmv_omp_f64(A.row_ptr, A.col, vals_stored, x_stored)
+    ya = O.spmv_abs_omp_f64(A.row_ptr, A.col, vals_stored, x_stored)
+    return component_error(y_gpu, ys, ya)
+
+
 def spmv_form(A, dtype: str, rp, col, vals64, x64, steps: int, dev, stream, peak: float,
-              workload: str) -> dict:
+              workload: str, cpu_check: bool = True) -> dict:
     """One tuned SpMV of A with values stored as `dtype` (x FP64 for FP64
     values, FP32 otherwise), timed over `steps` graph-captured launches, with
     its error against an FP64 SpMV (the OpenMP oracle) of the inputs as
@@ -401,8 +411,6 @@ def spmv_form(A, dtype: str, rp, col, vals64, x64, steps: int, dev, stream, peak
     import torch
 
     import merbit_b200 as mb
-    from oracle import oracle as O
-
     vt = {"f64": torch.float64, "f32": torch.float32, "bf16": torch.bfloat16}[dtype]
     xt = torch.float64 if dtype == "f64" else torch.float32
     vals = vals64.to(vt)
@@ -417,10 +425,7 @@ def spmv_form(A, dtype: str, rp, col, vals64, x64, steps: int, dev, stream, peak
     plan.check()
     B = alg_bytes(A, dtype)
     gbs = B / (ms * 1e-3) / 1e9
-    vs = vals.to(torch.float64).cpu().numpy()
-    xs = x.to(torch.float64).cpu().numpy()
-    ys, _ = O.spmv_omp_f64(A.row_ptr, A.col, vs, xs)
-    ya = O.spmv_abs_omp_f64(A.row_ptr, A.col, vs, xs)
+    y_gpu = y.cpu().numpy()
     out = {
         "ms": round(ms, 5), "gbs": round(gbs, 2), "gflops": round(2.0 * A.nnz / (ms * 1e-3) / 1e9, 2),
         "algorithmic_bytes": B,
@@ -431,9 +436,13 @@ def spmv_form(A, dtype: str, rp, col, vals64, x64, steps: int, dev, stream, peak
         "kernel": f"{KERNEL_OF_KIND[info.kind]} block={info.block} ipt={info.items_per_thread} "
                   f"tile_items={info.tile_items} l1_carveout={info.l1_carveout} "
                   f"gather_l2_only={int(info.gather_l2_only)}",
-        "err_vs_fp64_stored_inputs": component_error(y.cpu().numpy(), ys, ya),
         "clocks": clk,
     }
+    if cpu_check:
+        # CPU-baseline leg: the FP64 CPU SpMV (OpenMP restatement) of the
+        # values and x as stored, against which the error is taken
+        out["err_vs_fp64_stored_inputs"] = cpu_fp64_error(
+            A, vals.to(torch.float64).cpu().numpy(), x.to(torch.float64).cpu().numpy(), y_gpu)
     plan.close()
     return out
 
@@ -624,7 +633,8 @@ def secondary_forms(args, A_zipf, rp, col, vals64, x64, dev, stream, peak,
     forms, ratios = {}, {}
     t0 = time.perf_counter()
     # precision form on the power-law matrix itself (same matrix, same k = 1)
-    zf = {d: spmv_form(A_zipf, d, rp, col, vals64, x64, steps, dev, stream, peak, "zipf_2m")
+    chk = not args.no_cpu_baseline
+    zf = {d: spmv_form(A_zipf, d, rp, col, vals64, x64, steps, dev, stream, peak, "zipf_2m", chk)
           for d in ("f32", "bf16")}
     forms["zipf_2m"] = zf
     # 5-point Laplacian 256^2, FP64 (L2-resident: 5.2 MB): back to back from
@@ -634,7 +644,7 @@ def secondary_forms(args, A_zipf, rp, col, vals64, x64, dev, stream, peak,
     lcol = torch.from_numpy(Lp.col).to(dev)
     lv = torch.from_numpy(Lp.vals).to(dev)
     lx = torch.from_numpy(synth.workload_x("laplace2d_256", Lp.ncol)).to(dev)
-    lap = spmv_form(Lp, "f64", lrp, lcol, lv, lx, steps, dev, stream, peak, "laplace2d_256")
+    lap = spmv_form(Lp, "f64", lrp, lcol, lv, lx, steps, dev, stream, peak, "laplace2d_256", chk)
     lap["l2"] = "L2-resident between back-to-back launches (ms, gbs); ms_l2_flushed flushes L2"
     lap["ms_l2_flushed"] = round(l2_flushed_ms(Lp, lrp, lcol, lv, lx, dev, stream), 5)
     forms["laplace2d_256"] = {"nrow": Lp.nrow, "nnz": Lp.nnz, "f64": lap}
@@ -645,7 +655,7 @@ def secondary_forms(args, A_zipf, rp, col, vals64, x64, dev, stream, peak,
     scol = torch.from_numpy(S.col).to(dev)
     sv = torch.from_numpy(S.vals).to(dev)
     sx = torch.from_numpy(synth.workload_x("stencil27_160", S.ncol)).to(dev)
-    st = {d: spmv_form(S, d, srp, scol, sv, sx, steps, dev, stream, peak, "stencil27_160")
+    st = {d: spmv_form(S, d, srp, scol, sv, sx, steps, dev, stream, peak, "stencil27_160", chk)
           for d in ("f64", "f32", "bf16")}
     forms["stencil27_160"] = {"nrow": S.nrow, "nnz": S.nnz, **st}
     del srp, scol, sv, sx, S
@@ -663,16 +673,18 @@ def secondary_forms(args, A_zipf, rp, col, vals64, x64, dev, stream, peak,
     forms["wall_s"] = round(time.perf_counter() - t0, 1)
 
     def ratio(plain_ms, mixed_ms, err, what):
+        # err is None when the CPU-baseline leg (and its FP64 check) is off
         return {"speedup": round(plain_ms / mixed_ms, 3), "plain_f64_ms": plain_ms,
-                "mixed_ms": mixed_ms, "err_max": err["max"], "err_median": err["median"],
-                "within_1e-6": bool(err["max"] <= 1e-6), "compares": what}
+                "mixed_ms": mixed_ms, "err_max": err["max"] if err else None,
+                "err_median": err["median"] if err else None,
+                "within_1e-6": bool(err["max"] <= 1e-6) if err else None, "compares": what}
 
     for d in ("f32", "bf16"):
         ratios[f"zipf_2m_{d}_vs_f64"] = ratio(
-            ms_headline, zf[d]["ms"], zf[d]["err_vs_fp64_stored_inputs"],
+            ms_headline, zf[d]["ms"], zf[d].get("err_vs_fp64_stored_inputs"),
             f"power-law 2M, k = 1: {d} values + f32 x vs plain FP64, same matrix")
         ratios[f"stencil27_160_{d}_vs_f64"] = ratio(
-            st["f64"]["ms"], st[d]["ms"], st[d]["err_vs_fp64_stored_inputs"],
+            st["f64"]["ms"], st[d]["ms"], st[d].get("err_vs_fp64_stored_inputs"),
             f"27-point stencil 160^3, k = 1: {d} values + f32 x vs plain FP64, same matrix")
     for k in (1, 32):
         b = bf[f"k{k}"]
