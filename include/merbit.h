@@ -255,10 +255,12 @@ int merbit_batch_spmm(merbit_batch batch, double alpha, double beta, void* strea
 /* The batch autotuner.  Times the SpMM kernel at each tile size and RHS
  * vector width and, for k = 1 on 16-byte aligned arrays, the warp-tile
  * kernel in each variant; with the warp-tile kernel it then chooses the
- * items per lane (7, 11 or 15) per matrix signature class (mean row length
- * and longest-row skew), largest classes first, keeping whatever times
- * fastest for the whole launch.  The choices are cached per matrix
- * signature.  Synchronizes. */
+ * items per lane (7, 11, 15, 19 or 23, as the variant takes) per matrix
+ * signature class (mean row length and longest-row skew), largest classes
+ * first, keeping whatever times fastest for the whole launch; the choices
+ * are cached per matrix signature.  With the SpMM kernel at vector width 4
+ * it chooses in the same way, per class, between the two tile sizes of the
+ * winning size's pair (merbit_batch_set_matrix_tile).  Synchronizes. */
 int merbit_batch_tune(merbit_batch batch, void* stream);
 int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info);
 /* The configuration of matrix `index` of the batch (the reference fixes one
@@ -266,7 +268,8 @@ int merbit_batch_get_info(merbit_batch batch, merbit_batch_info* info);
  * merbit_batch_info), its merge items per tile and items per lane.  With
  * the warp-tile kernel (k = 1) each matrix has its own tile size, chosen by
  * merbit_batch_tune per matrix signature class and cached per signature
- * for later batches and plans of the process. */
+ * for later batches and plans of the process; with the SpMM kernel each
+ * matrix takes one of a pair of tile sizes (merbit_batch_set_matrix_tile). */
 int merbit_batch_get_matrix_config(merbit_batch batch, int32_t index, int32_t* kernel,
                                    int32_t* tile_items, int32_t* items_per_thread);
 /* Selects the batch's kernel by hand (as merbit_plan_set_config does for a
@@ -283,6 +286,13 @@ int merbit_batch_set_kernel(merbit_batch batch, int32_t kernel, int32_t option, 
  * arrays only, else MERBIT_ERR_UNSUPPORTED).  Synchronizes. */
 int merbit_batch_set_matrix_config(merbit_batch batch, int32_t index, int32_t items_per_thread,
                                    void* stream);
+/* Sets the merge items per tile of matrix `index` on the SpMM kernel (kernel
+ * 0, vector width 4, k = 4, 8, 16 or 32): the other tile of the pair the
+ * batch's tile size belongs to (256/512, or the two odd tiles of k).  One
+ * launch then runs matrices of both tile sizes; merbit_batch_tune chooses
+ * them per matrix signature class.  Synchronizes. */
+int merbit_batch_set_matrix_tile(merbit_batch batch, int32_t index, int32_t tile_items,
+                                 void* stream);
 int merbit_batch_destroy(merbit_batch batch);
 
 /* y[nrow] = alpha*A*x + beta*y without allocating any device memory -- for

@@ -97,6 +97,7 @@ SIGNATURES = {
     "merbit_batch_get_info": (C.c_int, [_P, _P]),
     "merbit_batch_get_matrix_config": (C.c_int, [_P, C.c_int32, _P, _P, _P]),
     "merbit_batch_set_matrix_config": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
+    "merbit_batch_set_matrix_tile": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
     "merbit_batch_set_kernel": (C.c_int, [_P, C.c_int32, C.c_int32, _P]),
     "merbit_batch_destroy": (C.c_int, [_P]),
     "merbit_spmv_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int,
@@ -464,15 +465,22 @@ class Batch:
         return out
 
     def set_kernel(self, kernel: int, option: int, stream=None) -> None:
-        """kernel 0: SpMM kernel with `option` (256/512) items per tile;
-        kernel 1: warp-tile kernel (k = 1) in variant `option` (0-2)."""
+        """kernel 0: SpMM kernel with `option` merge items per tile (256,
+        512 or an odd tile of k); kernel 1: warp-tile kernel (k = 1) in
+        variant `option` (0-9)."""
         _check(lib().merbit_batch_set_kernel(self._h, kernel, option, _stream_ptr(stream)))
 
     def set_matrix_config(self, index: int, items_per_thread: int, stream=None) -> None:
-        """Items per lane (7, 11, 15) of matrix `index` on the warp-tile
-        kernel (k = 1, aligned arrays)."""
+        """Items per lane (7, 11, 15, 19 or 23, as the variant takes) of
+        matrix `index` on the warp-tile kernel (k = 1, aligned arrays)."""
         _check(lib().merbit_batch_set_matrix_config(self._h, index, items_per_thread,
                                                     _stream_ptr(stream)))
+
+    def set_matrix_tile(self, index: int, tile_items: int, stream=None) -> None:
+        """Merge items per tile of matrix `index` on the SpMM kernel (k = 4,
+        8, 16, 32 at vector width 4): the other tile of the batch's pair."""
+        _check(lib().merbit_batch_set_matrix_tile(self._h, index, tile_items,
+                                                  _stream_ptr(stream)))
 
     def close(self) -> None:
         if self._h:

@@ -140,11 +140,12 @@ int spmm_block(merbit_plan_s* p, int kk, double alpha, const void* x, long long 
 // Batch of plans sharing one persistent launch.
 struct merbit_batch_s {
     int count = 0, k = 0, dtype = 0, items = 256, vw = 1;
-    // kernel 0: the SpMM kernel (items, vw for every matrix); kernel 1 (k = 1,
-    // 16-byte aligned arrays): the warp-tile kernel with variant `variant`
-    // and ipt[i] items per lane for matrix i
-    int kernel = 0, variant = 0;
-    std::vector<int> ipt;
+    // kernel 0: the SpMM kernel at vector width vw, matrix i with tiles of
+    // tile[i] merge items, each `items` or (items2 != 0, vw = 4) `items2`;
+    // kernel 1 (k = 1, 16-byte aligned arrays): the warp-tile kernel with
+    // variant `variant` and ipt[i] items per lane for matrix i
+    int kernel = 0, variant = 0, items2 = 0;
+    std::vector<int> ipt, tile;
     bool all_vec = true;
     int device = 0;
     std::vector<merbit_plan_s*> plans;
@@ -183,29 +184,66 @@ int batch_upload(merbit_batch_s* b, const std::vector<SpmmDesc>& h, long long to
     return MERBIT_OK;
 }
 
-// The SpMM kernel with `items` merge items per tile for every matrix.
-int batch_build(merbit_batch_s* b, int items, cudaStream_t s) {
-    std::vector<SpmmDesc> h(b->count);
-    long long tot = 0;
-    for (int i = 0; i < b->count; ++i) {
-        const Partition* part = nullptr;
-        int st = plan_partition(b->plans[i], items, &part, s);
-        if (st != MERBIT_OK) return st;
-        if (tot + part->num_tiles > INT_MAX) return fail(MERBIT_ERR_OVERFLOW, "batch: too many tiles");
-        h[i] = make_desc(b->plans[i], part, b->x[i], b->ldx[i], b->y[i], b->ldy[i], (int)tot);
-        tot += part->num_tiles;
-    }
+// Widest vector width every member allows at `items` merge items per tile.
+int batch_vw(const merbit_batch_s* b, int items) {
     int vw = 4;
     const int esz = (int)xy_size(b->dtype);
     for (int i = 0; i < b->count; ++i)
         vw = std::min(vw, pick_vw(b->k, b->ldx[i], b->x[i], b->y[i], b->ldy[i], esz, items));
-    if (!spmm_config_exists(b->k, vw, items)) vw = 1;
+    return spmm_config_exists(b->k, vw, items) ? vw : 1;
+}
+
+// The SpMM kernel, matrix i with tiles of tile[i] merge items (each `items`
+// or `items2`; items2 = 0: `items` for every matrix).
+int batch_build_tiles(merbit_batch_s* b, int items, int items2, const std::vector<int>& tile,
+                      cudaStream_t s) {
+    int vw = batch_vw(b, items);
+    if (items2) {
+        if (vw != 4 || batch_vw(b, items2) != 4 || !spmm_pair_exists(b->k, 4, items, items2))
+            return fail(MERBIT_ERR_UNSUPPORTED,
+                        "batch: no tile pair of these sizes for this k and these operands");
+    }
+    std::vector<SpmmDesc> h(b->count);
+    long long tot = 0;
+    for (int i = 0; i < b->count; ++i) {
+        const int ti = items2 && tile[i] == items2 ? items2 : items;
+        const Partition* part = nullptr;
+        int st = plan_partition(b->plans[i], ti, &part, s);
+        if (st != MERBIT_OK) return st;
+        if (tot + part->num_tiles > INT_MAX) return fail(MERBIT_ERR_OVERFLOW, "batch: too many tiles");
+        h[i] = make_desc(b->plans[i], part, b->x[i], b->ldx[i], b->y[i], b->ldy[i], (int)tot);
+        h[i].ipt = ti;
+        tot += part->num_tiles;
+    }
     int st = batch_upload(b, h, tot, s);
     if (st != MERBIT_OK) return st;
     b->kernel = 0;
     b->items = items;
+    b->items2 = items2;
+    b->tile.assign(b->count, items);
+    if (items2)
+        for (int i = 0; i < b->count; ++i) b->tile[i] = tile[i] == items2 ? items2 : items;
     b->vw = vw;
     return MERBIT_OK;
+}
+
+// The SpMM kernel with `items` merge items per tile for every matrix.
+int batch_build(merbit_batch_s* b, int items, cudaStream_t s) {
+    return batch_build_tiles(b, items, 0, {}, s);
+}
+
+// The tile pair (smaller, larger) that `items` belongs to at k, or false.
+bool tile_pair_of(int k, int items, int* lo, int* hi) {
+    int c[8];
+    const int n = spmm_tile_candidates(k, c);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+            if (spmm_pair_exists(k, 4, c[i], c[j]) && (items == c[i] || items == c[j])) {
+                *lo = c[i];
+                *hi = c[j];
+                return true;
+            }
+    return false;
 }
 
 // Nearest items per lane that `variant` takes.
@@ -233,6 +271,8 @@ int batch_build_warp(merbit_batch_s* b, int variant, cudaStream_t s) {
     b->kernel = 1;
     b->variant = variant;
     b->items = 0;
+    b->items2 = 0;
+    b->tile.clear();
     b->vw = 1;
     return MERBIT_OK;
 }
@@ -249,7 +289,7 @@ int batch_run(merbit_batch_s* b, double alpha, double beta, cudaStream_t s) {
     a.alpha = alpha;
     a.beta = beta;
     if (b->kernel == 1) return batch_warp_launch(b->dtype, b->variant, a, s);
-    return spmm_launch(b->dtype, b->k, b->vw, b->items, a, s);
+    return spmm_launch(b->dtype, b->k, b->vw, b->items, a, s, b->items2);
 }
 
 // Mean ms of one batch launch (2 warm-up launches, then `reps` timed).
@@ -482,11 +522,52 @@ int merbit_batch_tune(merbit_batch batch, void* stream) {
             for (int i = 0; i < batch->count; ++i)
                 tune_cache_store_batch_ipt(batch->plans[i], best_variant, batch->ipt[i]);
     }
+    // 3. SpMM kernel at vector width 4: the tile size per signature class,
+    //    between the two of the winning size's pair, one pass of coordinate
+    //    descent over the classes
+    int lo = 0, hi = 0;
+    std::vector<int> best_tile(batch->count, best_items);
+    bool paired = false;
+    if (st == MERBIT_OK && best_kernel == 0 && best_vw == 4 &&
+        tile_pair_of(batch->k, best_items, &lo, &hi)) {
+        std::map<int, long long> class_nnz;
+        for (auto* p : batch->plans) class_nnz[batch_class(p)] += p->nnz;
+        std::vector<std::pair<long long, int>> order;
+        for (auto& kv : class_nnz) order.push_back({-kv.second, kv.first});
+        std::sort(order.begin(), order.end());
+        std::vector<int> cur = best_tile;
+        for (auto& oc : order) {
+            const int cls = oc.second;
+            std::vector<int> trial = cur;
+            const int other = best_items == lo ? hi : lo;
+            bool any = false;
+            for (int i = 0; i < batch->count; ++i)
+                if (batch_class(batch->plans[i]) == cls && trial[i] != other) {
+                    trial[i] = other;
+                    any = true;
+                }
+            if (!any) continue;
+            st = batch_build_tiles(batch, lo, hi, trial, s);
+            if (st == MERBIT_ERR_UNSUPPORTED) {
+                st = MERBIT_OK;  // the operands take no pair
+                break;
+            }
+            float ms = 0.f;
+            if (st == MERBIT_OK) st = time_batch(batch, s, e0, e1, 3, &ms);
+            if (st != MERBIT_OK) break;
+            if (ms < best) {
+                best = ms;
+                cur = trial;
+                paired = true;
+            }
+        }
+        best_tile = cur;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != MERBIT_OK) return st;
     if (best_kernel == 1) return batch_build_warp(batch, best_variant, s);
-    st = batch_build(batch, best_items, s);
+    st = paired ? batch_build_tiles(batch, lo, hi, best_tile, s) : batch_build(batch, best_items, s);
     if (st != MERBIT_OK) return st;
     batch->vw = best_vw;
     return MERBIT_OK;
@@ -533,6 +614,29 @@ int merbit_batch_set_matrix_config(merbit_batch batch, int32_t index, int32_t it
     return batch_build_warp(batch, variant, (cudaStream_t)stream);
 }
 
+int merbit_batch_set_matrix_tile(merbit_batch batch, int32_t index, int32_t tile_items,
+                                 void* stream) {
+    if (!batch) return fail(MERBIT_ERR_INVALID, "batch_set_matrix_tile: batch is null");
+    if (index < 0 || index >= batch->count)
+        return fail(MERBIT_ERR_INVALID, "batch_set_matrix_tile: index out of range");
+    if (batch->kernel != 0)
+        return fail(MERBIT_ERR_UNSUPPORTED,
+                    "batch_set_matrix_tile: the batch runs the warp-tile kernel (use "
+                    "merbit_batch_set_matrix_config, or merbit_batch_set_kernel(0, ...) first)");
+    int lo = 0, hi = 0;
+    if (batch->vw != 4 || !tile_pair_of(batch->k, batch->items, &lo, &hi) ||
+        (tile_items != lo && tile_items != hi))
+        return fail(MERBIT_ERR_INVALID,
+                    "batch_set_matrix_tile: at vector width 4, k = 4, 8, 16 or 32, a matrix may "
+                    "take the other tile of the batch's pair (256/512, or the two odd tiles of k)");
+    std::vector<int> tile = batch->tile;
+    tile[index] = tile_items;
+    bool uniform = true;
+    for (int t : tile) uniform = uniform && t == tile[0];
+    if (uniform) return batch_build(batch, tile[0], (cudaStream_t)stream);
+    return batch_build_tiles(batch, lo, hi, tile, (cudaStream_t)stream);
+}
+
 int merbit_batch_get_matrix_config(merbit_batch batch, int32_t index, int32_t* kernel,
                                    int32_t* tile_items, int32_t* items_per_thread) {
     if (!batch || !kernel || !tile_items || !items_per_thread)
@@ -544,8 +648,8 @@ int merbit_batch_get_matrix_config(merbit_batch batch, int32_t index, int32_t* k
         *items_per_thread = batch->ipt[index];
         *tile_items = 32 * batch->ipt[index];
     } else {
-        *tile_items = batch->items;
-        *items_per_thread = batch->items / 32;
+        *tile_items = batch->tile.empty() ? batch->items : batch->tile[index];
+        *items_per_thread = *tile_items / 32;
     }
     return MERBIT_OK;
 }

@@ -568,7 +568,12 @@ struct SpmmLaunch {
 
 // Launches the SpMM kernel for k right-hand sides, vw values per lane and
 // `items` merge items per warp tile.
-int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s);
+// items2 != 0: a batch whose matrices take tiles of `items` or `items2`
+// (descriptor field ipt = the matrix's tile items); pairs exist for vector
+// width 4 at k = 4, 8, 16, 32: (256, 512) and the two odd tiles of k.
+int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s,
+                int items2 = 0);
+bool spmm_pair_exists(int k, int vw, int items, int items2);
 
 // Batched warp-tile SpMV for k = 1 (batch_warp.cu): every descriptor's
 // tiles hold 32 * ipt merge items, ipt one of kBatchIpts; variant indexes

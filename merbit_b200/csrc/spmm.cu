@@ -631,16 +631,31 @@ struct SpmmTile {
     }
 };
 
-template <int DT, int K, int VW, int ITEMS, int WARPS, bool DV>
+// The stage of a warp when a launch takes tiles of ITEMS or ITEMS2 items
+// (ITEMS2 = 0: ITEMS only): large enough for either, one mbarrier after both.
+template <int DT, int K, int VW, int ITEMS, int ITEMS2, bool DV>
+struct SpmmStage {
+    using T1 = SpmmTile<DT, K, VW, ITEMS, DV>;
+    using T2 = SpmmTile<DT, K, VW, ITEMS2 ? ITEMS2 : ITEMS, DV>;
+    static constexpr size_t bar_offset =
+        T1::bar_offset > T2::bar_offset ? T1::bar_offset : T2::bar_offset;
+    static constexpr size_t bytes = bar_offset + 16;
+};
+
+// ITEMS2 != 0: a batch whose matrices take tiles of either size; descriptor
+// field `ipt` holds the tile items of its matrix (0 or ITEMS: ITEMS).
+template <int DT, int K, int VW, int ITEMS, int ITEMS2, int WARPS, bool DV>
 __global__ void __launch_bounds__(WARPS * 32) spmm_kernel(const SpmmLaunch a) {
-    using T = SpmmTile<DT, K, VW, ITEMS, DV>;
+    using St = SpmmStage<DT, K, VW, ITEMS, ITEMS2, DV>;
+    using T = typename St::T1;
+    using T2 = typename St::T2;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned s_epoch;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_epoch = *(volatile unsigned*)&a.state->epoch;
-    unsigned char* ws = smem + (size_t)warp * T::bytes;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(ws + T::bar_offset);
+    unsigned char* ws = smem + (size_t)warp * St::bytes;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ws + St::bar_offset);
     if (lane == 0) {
         mbar_init(bar, 1);
         fence_mbar_init();
@@ -662,11 +677,20 @@ __global__ void __launch_bounds__(WARPS * 32) spmm_kernel(const SpmmLaunch a) {
         }
         const SpmmDesc& d = *dp;
         const int lt = u - d.tile_begin;
-        T::issue(d, lt, ws, bar, lane, a.dv_perm);
+        const bool second = ITEMS2 != 0 && d.ipt == ITEMS2;  // warp-uniform
+        if (second)
+            T2::issue(d, lt, ws, bar, lane, a.dv_perm);
+        else
+            T::issue(d, lt, ws, bar, lane, a.dv_perm);
         const bool ok = __all_sync(0xFFFFFFFFu, mbar_wait_bounded(bar, phase, a.state));
         phase ^= 1u;
         __syncwarp();
-        if (ok) T::process(a, d, u, lt, epoch, ws, lane);
+        if (ok) {
+            if (second)
+                T2::process(a, d, u, lt, epoch, ws, lane);
+            else
+                T::process(a, d, u, lt, epoch, ws, lane);
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) finish_launch(a.state, epoch);
@@ -674,15 +698,14 @@ __global__ void __launch_bounds__(WARPS * 32) spmm_kernel(const SpmmLaunch a) {
 
 namespace {
 
-template <int DT, int K, int VW, int ITEMS, int WARPS, bool DV>
+template <int DT, int K, int VW, int ITEMS, int WARPS, bool DV, int ITEMS2 = 0>
 int launch_spmm_cfg(const SpmmLaunch& a, cudaStream_t s) {
-    using T = SpmmTile<DT, K, VW, ITEMS, DV>;
-    constexpr size_t smem = T::bytes * WARPS;
+    constexpr size_t smem = SpmmStage<DT, K, VW, ITEMS, ITEMS2, DV>::bytes * WARPS;
     static int grid_cap[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 64) return fail(MERBIT_ERR_UNSUPPORTED, "spmm: device ordinal >= 64");
-    auto kern = spmm_kernel<DT, K, VW, ITEMS, WARPS, DV>;
+    auto kern = spmm_kernel<DT, K, VW, ITEMS, ITEMS2, WARPS, DV>;
     // per-device cache; threads that race here compute the same value
     int cap = __atomic_load_n(&grid_cap[dev], __ATOMIC_ACQUIRE);
     if (cap == 0) {
@@ -715,9 +738,26 @@ int launch_spmm_cfg(const SpmmLaunch& a, cudaStream_t s) {
 
 // Configurations: (K, VW, ITEMS).  WARPS = 4.
 template <int DT>
-int launch_spmm_dt(int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s) {
+int launch_spmm_dt(int k, int vw, int items, int items2, const SpmmLaunch& a, cudaStream_t s) {
     constexpr bool kDv = DT != MERBIT_BF16;  // fused dval: F64 and F32 plans
     if (a.dv_out && !kDv) return fail(MERBIT_ERR_UNSUPPORTED, "spmm: fused dval needs F64 or F32 values");
+    if (items2) {
+        // batches whose matrices take either of two tile sizes (vector width 4)
+        if (a.dv_out) return fail(MERBIT_ERR_UNSUPPORTED, "spmm: tile pairs take no fused dval");
+#define MERBIT_SPMM_PAIR(KK, I1, I2) \
+        if (k == KK && vw == 4 && items == I1 && items2 == I2) \
+            return launch_spmm_cfg<DT, KK, 4, I1, 4, false, I2>(a, s);
+        MERBIT_SPMM_PAIR(4, 256, 512)
+        MERBIT_SPMM_PAIR(4, 288, 480)
+        MERBIT_SPMM_PAIR(8, 256, 512)
+        MERBIT_SPMM_PAIR(8, 272, 496)
+        MERBIT_SPMM_PAIR(16, 256, 512)
+        MERBIT_SPMM_PAIR(16, 264, 504)
+        MERBIT_SPMM_PAIR(32, 256, 512)
+        MERBIT_SPMM_PAIR(32, 260, 508)
+#undef MERBIT_SPMM_PAIR
+        return fail(MERBIT_ERR_INVALID, "spmm: no such tile pair");
+    }
 #define MERBIT_SPMM_CASE(KK, VV, II)                                                  \
     if (k == KK && vw == VV && items == II)                                           \
         return a.dv_out ? launch_spmm_cfg<DT, KK, VV, II, 4, kDv>(a, s)                \
@@ -806,12 +846,19 @@ int spmm_odd_tile(int k) {
     return 0;
 }
 
-int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s) {
+bool spmm_pair_exists(int k, int vw, int items, int items2) {
+    if (vw != 4 || !(k == 4 || k == 8 || k == 16 || k == 32)) return false;
+    if (items == 256 && items2 == 512) return true;
+    return items2 == spmm_odd_tile(k) && items == (k == 4 ? 288 : k == 8 ? 272 : k == 16 ? 264 : 260);
+}
+
+int spmm_launch(int dtype, int k, int vw, int items, const SpmmLaunch& a, cudaStream_t s,
+                int items2) {
     if (a.total_tiles <= 0) return MERBIT_OK;
     switch (dtype) {
-    case MERBIT_F64: return launch_spmm_dt<MERBIT_F64>(k, vw, items, a, s);
-    case MERBIT_F32: return launch_spmm_dt<MERBIT_F32>(k, vw, items, a, s);
-    case MERBIT_BF16: return launch_spmm_dt<MERBIT_BF16>(k, vw, items, a, s);
+    case MERBIT_F64: return launch_spmm_dt<MERBIT_F64>(k, vw, items, items2, a, s);
+    case MERBIT_F32: return launch_spmm_dt<MERBIT_F32>(k, vw, items, items2, a, s);
+    case MERBIT_BF16: return launch_spmm_dt<MERBIT_BF16>(k, vw, items, items2, a, s);
     }
     return fail(MERBIT_ERR_INVALID, "spmm: bad dtype");
 }
