@@ -12,11 +12,19 @@
 // so that one tile walk serves a single matrix and the matrices of a batch.
 #pragma once
 
+#include <type_traits>
+
 #include "merbit_internal.cuh"
 
 namespace merbit {
 
 constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// Products per TwoSum step on single-row tiles with compensated (FP32/BF16)
+// accumulation: a block of 4 is summed by f32 fused multiply-adds (at most
+// 4 roundings of the block's sum |a x|), then added exactly.
+template <class Acc>
+constexpr int kWarpBlockSum = std::is_same<Acc, AccTwoSum>::value ? 4 : 1;
 
 // One stage of a warp: row_ptr window (RP entries; warp_rp_cap(IPT) by
 // default -- the plan only runs such a configuration when no tile ends more
@@ -145,6 +153,9 @@ struct WarpTile {
     static_assert(32 * IPT <= S::W, "stage smaller than the tile");
     static constexpr int GV = 16 / (int)sizeof(V);
     static constexpr int kOutCap = S::OUTCAP;
+    // single-row tiles with compensated (TwoSum) accumulation: products
+    // enter in blocks of this many, fused in f32 (1: one TwoSum each)
+    static constexpr int kBlockSum = kWarpBlockSum<Acc>;
 
     // Issues the copies of tile u into stage `ws`; lane 0 arms the barrier
     // with the byte count before any copy is issued.
@@ -208,10 +219,25 @@ struct WarpTile {
             }
             Acc acc;
             acc.zero();
+            if constexpr (kBlockSum > 1) {
+                // blocks of kBlockSum products summed by fused multiply-adds,
+                // each block added to (s, c) by TwoSum
 #pragma unroll
-            for (int j = 0; j < IPT; ++j) {
-                const int i = lane + 32 * j;
-                if (i < nz) acc.add(to_p(s_val[x0 + i - val_base]) * (P)xg[j]);
+                for (int j0 = 0; j0 < IPT; j0 += kBlockSum) {
+                    P blk = (P)0;
+#pragma unroll
+                    for (int j = j0; j < j0 + kBlockSum && j < IPT; ++j) {
+                        const int i = lane + 32 * j;
+                        if (i < nz) blk = fmaf(to_p(s_val[x0 + i - val_base]), (P)xg[j], blk);
+                    }
+                    acc.add(blk);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < IPT; ++j) {
+                    const int i = lane + 32 * j;
+                    if (i < nz) acc.add(to_p(s_val[x0 + i - val_base]) * (P)xg[j]);
+                }
             }
             double v = acc.value();
 #pragma unroll
