@@ -20,9 +20,10 @@ namespace merbit {
 
 constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
-// Products per TwoSum step on single-row tiles with compensated (FP32/BF16)
-// accumulation: a block of 4 is summed by f32 fused multiply-adds (at most
-// 4 roundings of the block's sum |a x|), then added exactly.
+// Products per TwoSum step with compensated (FP32/BF16) accumulation: on a
+// single-row tile a block of 4 is summed by f32 fused multiply-adds, on the
+// walk the products of 4 steps are summed in f32; either way a block costs
+// at most 4 roundings of its sum |a x| and is then added exactly.
 template <class Acc>
 constexpr int kWarpBlockSum = std::is_same<Acc, AccTwoSum>::value ? 4 : 1;
 
@@ -309,8 +310,12 @@ struct WarpTile {
         int ly = lo, lx = dl - lo;
 
         // ---- walk IPT items: predicated steps, completed rows staged
+        // (compensated accumulation: the products of every kBlockSum steps
+        // are summed in f32 and added by one TwoSum; a row end adds the
+        // open block's sum in double)
         Acc acc;
         acc.zero();
+        P blk = (P)0;
         int first_row = -1;
         double first_val = 0.0;
         int next_end = ly < nr ? s_rp[rpo + ly + 1] - x0 : INT_MAX;
@@ -320,7 +325,8 @@ struct WarpTile {
             const bool is_end = valid && lx >= next_end;
             const P p = (valid && !is_end) ? s_prod[pofs + lx] : (P)0;
             if (is_end) {
-                const double v = acc.value();
+                const double v = kBlockSum > 1 ? acc.value() + (double)blk : acc.value();
+                blk = (P)0;
                 if (first_row < 0) {
                     first_row = ly;
                     first_val = v;
@@ -333,13 +339,21 @@ struct WarpTile {
                 ++ly;
                 next_end = ly < nr ? s_rp[rpo + ly + 1] - x0 : INT_MAX;
             }
-            acc.add(p);
+            if constexpr (kBlockSum > 1) {
+                blk += p;
+                if (i % kBlockSum == kBlockSum - 1) {
+                    acc.add(blk);
+                    blk = (P)0;
+                }
+            } else {
+                acc.add(p);
+            }
             lx += (valid && !is_end) ? 1 : 0;
         }
 
         // ---- warp segmented scan of (has_end, trailing partial)
         int f = first_row >= 0;
-        double v = acc.value();
+        double v = kBlockSum > 1 ? acc.value() + (double)blk : acc.value();
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const double vv = __shfl_up_sync(0xFFFFFFFFu, v, o);
