@@ -1314,6 +1314,28 @@ def competitors(A, rp, col, v, xd, yd, zd, B, dev, y_cpu):
                                     "via": "torch.mv on a torch.sparse_csr_tensor (cuSPARSE SpMV)"}
     except RuntimeError as e:  # a torch build without sparse CSR on CUDA
         res["cusparse_csr_spmv"] = {"unavailable": str(e).splitlines()[0][:120]}
+    # the same in FP32 (values and x f32, 32-bit indices, cuSPARSE's plain
+    # FP32 accumulation), beside this library's FP32 precision form
+    try:
+        A32 = torch.sparse_csr_tensor(rp, col, v.float(), size=(A.nrow, A.ncol))
+        x32 = xd.float()
+        for _ in range(3):
+            torch.mv(A32, x32)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(50):
+            torch.mv(A32, x32)
+        e1.record(s)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / 50
+        B32 = alg_bytes(A, "f32")
+        res["cusparse_csr_spmv_f32"] = {"value": round(B32 / (ms * 1e-3) / 1e9, 2), "unit": "GB/s",
+                                        "ms_per_spmv": round(ms, 5),
+                                        "via": "torch.mv, FP32 values and x, int32 indices"}
+        del A32, x32
+    except RuntimeError as e:
+        res["cusparse_csr_spmv_f32"] = {"unavailable": str(e).splitlines()[0][:120]}
     res.update(library_competitors(A, rp, col, v, xd, B, dev, y_cpu))
     return res
 
