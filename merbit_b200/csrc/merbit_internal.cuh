@@ -228,8 +228,8 @@ __device__ __forceinline__ double look_back(const int2* coords, const unsigned l
 // Precision policies.
 //   F64 : values, x, y, products and accumulation in double (plain form).
 //   F32 : values f32, x f32, products f32, two-sum (s, c) accumulation
-//         (single-row warp tiles add blocks of 4 products, fused in f32,
-//         per two-sum step; warp_tile.cuh).
+//         (the warp tiles and row groups add blocks of 4 products, summed
+//         in f32, per two-sum step; warp_tile.cuh, spmv_rows.cu).
 //   BF16: values bf16, otherwise as F32.
 // Carries between threads and tiles are always double.
 // ---------------------------------------------------------------------------

@@ -12,6 +12,8 @@
 //
 // The tuner (merbit_plan_tune) times this kernel beside the merge-path ones
 // and keeps it only where it wins; long rows make it slow, never wrong.
+#include <type_traits>
+
 #include "merbit_internal.cuh"
 
 namespace merbit {
@@ -67,6 +69,11 @@ __device__ __forceinline__ void finish_residual_only(LaunchState* st, double v, 
 // staging (j, j + LPR, ... of its row).  Every col/vals line is touched once
 // per warp instead of once per unrolled step, which cuts the L1 wavefronts of
 // short rows several-fold.  Blocks that do not fit take the strided path.
+// Products per TwoSum step with compensated (FP32/BF16) accumulation; a
+// block of 4 costs at most 4 roundings of its sum |a x|.
+template <class Acc>
+constexpr int kRowsBlock = std::is_same<Acc, AccTwoSum>::value ? 4 : 1;
+
 template <int DT, int LPR, int WARPS, bool RES, bool CG, bool STG = false>
 __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch a) {
     using Pr = Prec<DT>;
@@ -125,7 +132,13 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch 
                 __syncwarp();
                 // (clamped to the staged run, which a valid CSR never leaves)
                 const int i1 = min(e, be) - bs;
-                for (int i = max(s - bs, 0) + jl; i < i1; i += LPR) acc.add(sp[i]);
+                int i = max(s - bs, 0) + jl;
+                if constexpr (kRowsBlock<Acc> > 1) {
+                    // compensated accumulation: 4 products per TwoSum step
+                    for (; i + 3 * LPR < i1; i += 4 * LPR)
+                        acc.add((sp[i] + sp[i + LPR]) + (sp[i + 2 * LPR] + sp[i + 3 * LPR]));
+                }
+                for (; i < i1; i += LPR) acc.add(sp[i]);
                 __syncwarp();  // the slice is rewritten by the next block
                 staged = true;
             }
@@ -147,9 +160,22 @@ __global__ void __launch_bounds__(WARPS * 32) spmv_rows_kernel(const SpmvLaunch 
 #pragma unroll
                 for (int u = 0; u < UNR; ++u)
                     xg[u] = c[u] >= 0 ? (CG ? __ldcg(xv + c[u]) : __ldg(xv + c[u])) : (X)0;
+                if constexpr (kRowsBlock<Acc> > 1) {
+                    // compensated accumulation: blocks of 4 products summed
+                    // by f32 fused multiply-adds, one TwoSum per block
 #pragma unroll
-                for (int u = 0; u < UNR; ++u)
-                    if (c[u] >= 0) acc.add(to_p(v[u]) * (P)xg[u]);
+                    for (int u0 = 0; u0 < UNR; u0 += 4) {
+                        P blk = (P)0;
+#pragma unroll
+                        for (int u = u0; u < u0 + 4 && u < UNR; ++u)
+                            if (c[u] >= 0) blk = fmaf(to_p(v[u]), (P)xg[u], blk);
+                        acc.add(blk);
+                    }
+                } else {
+#pragma unroll
+                    for (int u = 0; u < UNR; ++u)
+                        if (c[u] >= 0) acc.add(to_p(v[u]) * (P)xg[u]);
+                }
             }
         }
         double t = acc.value();
