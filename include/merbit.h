@@ -129,8 +129,10 @@ int merbit_plan_set_values(merbit_plan plan, const void* d_vals);
 
 /* Selects the SpMV kernel configuration by timing the candidates on this
  * matrix (`x`,`y` are scratch vectors of the plan's dtype, contents
- * overwritten).  The choice is cached per matrix signature for the process.
- * Not capturable (it synchronizes). */
+ * overwritten): every usable configuration once (5 launches), then the
+ * three fastest in three rounds of 10 launches, keeping the best time.  The
+ * choice is cached per matrix signature for the process.  Not capturable
+ * (it synchronizes). */
 int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream);
 
 /* Kernel configurations the tuner chooses from, for a dtype: kind 0 = CTA

@@ -516,30 +516,48 @@ int merbit_plan_tune(merbit_plan plan, const void* d_x, void* d_y, void* stream)
     MERBIT_CUDA(cudaEventCreate(&e1));
     const int n = spmv_num_configs(plan->dtype);
     int best = plan->cfg;
-    float best_ms = 1e30f;
     int st = MERBIT_OK;
+    // ms of `reps` back-to-back launches of configuration c
+    auto time_cfg = [&](int c, int reps, float* ms) -> int {
+        int rc = MERBIT_OK;
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps && rc == MERBIT_OK; ++r) rc = run_spmv(plan, c, 1.0, d_x, 0.0, d_y, s);
+        cudaEventRecord(e1, s);
+        cudaError_t ce = cudaEventSynchronize(e1);
+        if (ce != cudaSuccess) return cuda_fail(ce, "plan_tune");
+        if (rc != MERBIT_OK) return rc;
+        cudaEventElapsedTime(ms, e0, e1);
+        *ms /= (float)reps;
+        return MERBIT_OK;
+    };
+    // 1. every usable configuration, 5 launches after 2 warm-up launches
+    std::vector<std::pair<float, int>> timed;
     for (int c = 0; c < n && st == MERBIT_OK; ++c) {
         bool ok = false;
         st = plan_config_ok(plan, c, &ok, s);
         if (st != MERBIT_OK) break;
         if (!ok) continue;
         for (int w = 0; w < 2 && st == MERBIT_OK; ++w) st = run_spmv(plan, c, 1.0, d_x, 0.0, d_y, s);
-        if (st != MERBIT_OK) break;
-        const int reps = 5;
-        cudaEventRecord(e0, s);
-        for (int r = 0; r < reps && st == MERBIT_OK; ++r) st = run_spmv(plan, c, 1.0, d_x, 0.0, d_y, s);
-        cudaEventRecord(e1, s);
-        cudaError_t ce = cudaEventSynchronize(e1);
-        if (ce != cudaSuccess) {
-            st = cuda_fail(ce, "plan_tune");
-            break;
-        }
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = c;
-        }
+        if (st == MERBIT_OK) st = time_cfg(c, 5, &ms);
+        if (st == MERBIT_OK) timed.push_back({ms, c});
+    }
+    // 2. the three fastest again, best of three rounds of 10 launches each
+    //    (a single short round cannot separate entries within a few percent)
+    if (st == MERBIT_OK && !timed.empty()) {
+        std::stable_sort(timed.begin(), timed.end());
+        const size_t top = std::min<size_t>(3, timed.size());
+        float best_ms = 1e30f;
+        best = timed[0].second;
+        for (int round = 0; round < 3 && st == MERBIT_OK; ++round)
+            for (size_t i = 0; i < top && st == MERBIT_OK; ++i) {
+                float ms = 0.f;
+                st = time_cfg(timed[i].second, 10, &ms);
+                if (st == MERBIT_OK && ms < best_ms) {
+                    best_ms = ms;
+                    best = timed[i].second;
+                }
+            }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
