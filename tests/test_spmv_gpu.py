@@ -78,6 +78,38 @@ def test_spmv_every_config(dtype, workload):
     assert O.rel_error(y.cpu().numpy(), yo, ya)[0] <= TOL[dtype]
 
 
+# The precision form's bound per row: products rounded to f32 (1 unit),
+# blocks of 4 of them summed in f32 before each TwoSum (3 units), and y
+# rounded to f32 on the store (1 unit): 5 units of sum |a x|.
+F32_FORM_BOUND = 5 * 2.0 ** -24
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_precision_form_error_bound(dtype):
+    """Positive values and x (no cancellation, so the bound is tight
+    relative to |y|): every configuration stays within 5 units of sum |a x|
+    per row, on single-row tiles (one row of 100,000 entries), the walk
+    (rows of 37), a power-law matrix and the row groups (stencil)."""
+    mats = [csr_from_lengths([100_000], ncol=150_000, seed=5),
+            csr_from_lengths([37] * 3_000, ncol=20_000, seed=6),
+            synth.workload("zipf_small"), synth.workload("stencil27_small")]
+    for A in mats:
+        A = synth.CSR(A.row_ptr, A.col, 0.5 + 0.5 * np.abs(np.tanh(A.vals)), A.ncol, A.name)
+        x = (0.5 + 0.5 * synth.uniform(9, A.ncol, 0.0, 1.0)).astype(np.float32)
+        yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+        rp, col, v = to_cuda(A, dtype)
+        plan = mb.Plan(rp, col, v, ncol=A.ncol)
+        xd = torch.from_numpy(x).cuda()
+        for idx, kind, block, ipt in plan.configs():
+            plan.set_config(idx)
+            y = plan.spmv(xd)
+            torch.cuda.synchronize()
+            emax = O.rel_error(y.cpu().numpy(), yo, ya)[0]
+            assert emax <= F32_FORM_BOUND, (A.name, idx, kind, ipt, emax)
+        plan.close()
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
 def test_alpha_beta(dtype):
