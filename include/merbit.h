@@ -247,7 +247,12 @@ typedef struct merbit_batch_info {
 /* A batch of `count` plans (same dtype) multiplied by k in {1,2,4,8,16,32}
  * right-hand sides in ONE persistent launch.  The X/Y device buffers of
  * each matrix are bound at creation (callers refill them between runs);
- * plans and buffers must outlive the batch.  Synchronizes. */
+ * plans and buffers must outlive the batch.  Untuned, it starts from the
+ * configurations that won on a 128-matrix R-MAT batch: at k = 1 the
+ * warp-tile kernel (variant 6, or the cached choices of the members'
+ * signatures), at k = 2 352-item staged-product tiles, at k >= 4 the odd
+ * tile of k at vector width 4 (where the operands allow them).
+ * Synchronizes. */
 int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* plans, int32_t k,
                         const void* const* d_x, const int64_t* ldx, void* const* d_y,
                         const int64_t* ldy, void* stream);

@@ -426,7 +426,19 @@ int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* p
         st = batch_build_warp(b, variant, (cudaStream_t)stream);
     } else {
         if (k == 1) b->ipt.assign(count, kBatchDefaultIpt);
-        st = batch_build(b, kDefaultItems, (cudaStream_t)stream);
+        // untuned SpMM batches start from the tile the tuner picked on the
+        // 128-matrix R-MAT batch: at vector width 4 the odd tile of k (480,
+        // 496, 504, 508 items at k = 4, 8, 16, 32; 2.38 against 3.24 ms at
+        // k = 4 for 256), at k = 2 the staged products in 352-item tiles
+        // (2.10 against 2.85 ms), else 256
+        int items = kDefaultItems;
+        if (k >= 4) {
+            const int odd = spmm_odd_tile(k);
+            if (odd && batch_vw(b, odd) == 4) items = odd;
+        } else if (k == 2 && batch_vw(b, 352) == 2) {
+            items = 352;
+        }
+        st = batch_build(b, items, (cudaStream_t)stream);
     }
     if (st != MERBIT_OK) {
         merbit_batch_destroy(b);
