@@ -68,6 +68,10 @@ def parse_args():
     ap.add_argument("--k", type=int, default=8,
                     help="right-hand sides of the batched form (--workload rmat_batch128)")
     ap.add_argument("--batch", type=int, default=128, help="matrices of the batched form")
+    ap.add_argument("--batch-tile", type=int, default=0,
+                    help="batched form: run the SpMM kernel with this many merge items per "
+                         "tile for every matrix (merbit_batch_set_kernel) instead of the "
+                         "default or tuned choice")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the secondary forms (stencil precision form, batched form, "
                          "differentiation form) that the default power-law run adds")
@@ -993,7 +997,9 @@ def run_batch(args):
         Xd.append(torch.from_numpy(X).to(dev))
         Yd.append(torch.empty(A.nrow, k, dtype=torch.float32, device=dev))
     batch = mb.Batch(plans, Xd, Yd)
-    if not args.no_tune:
+    if args.batch_tile:
+        batch.set_kernel(0, args.batch_tile)
+    elif not args.no_tune:
         batch.tune()
     info = batch.info()
     per_matrix = {}
