@@ -261,7 +261,8 @@ int merbit_batch_create(merbit_batch* batch, int32_t count, const merbit_plan* p
 int merbit_batch_spmm(merbit_batch batch, double alpha, double beta, void* stream);
 /* The batch autotuner.  Times the SpMM kernel at each tile size and RHS
  * vector width and, for k = 1 on 16-byte aligned arrays, the warp-tile
- * kernel in each variant; with the warp-tile kernel it then chooses the
+ * kernel in each variant (3 launches each, then the three fastest again in
+ * two rounds of 8); with the warp-tile kernel it then chooses the
  * items per lane (7, 11, 15, 19 or 23, as the variant takes) per matrix
  * signature class (mean row length and longest-row skew), largest classes
  * first, keeping whatever times fastest for the whole launch; the choices
