@@ -171,7 +171,10 @@ struct WarpTile {
         const V* vals = static_cast<const V*>(src.vals());
         const int nnz = src.nnz();
         const int nrp = src.nrow() + 1;
-        const unsigned tot = bulk_bytes(c0.y, c1.y + 1, nrp, 4, 4) +
+        // a tile inside one row stages no row_ptr window (process reads its
+        // one entry, row_ptr[y0], from global memory)
+        const bool single = c0.y == c1.y;
+        const unsigned tot = (single ? 0u : bulk_bytes(c0.y, c1.y + 1, nrp, 4, 4)) +
                              bulk_bytes(c0.x, c1.x, nnz, 4, 4) +
                              bulk_bytes(c0.x, c1.x, nnz, GV, (int)sizeof(V));
         __syncwarp();
@@ -182,7 +185,7 @@ struct WarpTile {
             mbar_arrive_expect_tx(bar, tot);
         }
         const uint64_t pol = l2_evict_first_policy();
-        stage_range<int>(s_rp, src.row_ptr(), c0.y, c1.y + 1, nrp, bar, pol, lane);
+        if (!single) stage_range<int>(s_rp, src.row_ptr(), c0.y, c1.y + 1, nrp, bar, pol, lane);
         stage_range<int>(s_col, src.col(), c0.x, c1.x, nnz, bar, pol, lane);
         stage_range<V>(s_val, vals, c0.x, c1.x, nnz, bar, pol, lane);
     }
@@ -204,13 +207,15 @@ struct WarpTile {
         const int x0 = c0.x, y0 = c0.y, x1 = c1.x, y1 = c1.y;
         const int nz = x1 - x0, nr = y1 - y0, L = nz + nr;
         const int rp_base = y0 & ~3, col_base = x0 & ~3, val_base = x0 & ~(GV - 1);
-        const int rpo0 = y0 - rp_base;  // staged index of row_ptr[y0]
 
         // ---- tile inside one row (no row ends: the common case for long rows
         // of power-law matrices, the reference's fast_track,
         // include/tile.cuh:267-290): the tile's partial is just the sum of
         // its products -- lane sums in a fixed order, then a butterfly.
         if (nr == 0) {
+            // start of row y0 (not staged for a single-row tile), loaded now
+            // so that it arrives while the gathers are in flight
+            const int rs1 = lane == 31 ? __ldg(src.row_ptr() + y0) : 0;
             const X* __restrict__ xv = static_cast<const X*>(src.x());
             X xg[IPT];
 #pragma unroll
@@ -248,7 +253,6 @@ struct WarpTile {
             if (lane == 31) {
                 publish_carry(src.slots(), src.nslots(), epoch, src.slot_base() + u, v);
                 // the row may have begun in this tile and end in the next
-                const int rs1 = s_rp[rpo0];
                 if (y1 < src.nrow() && u + 1 < src.num_tiles() && rs1 >= x0 && rs1 < x1) {
                     pa.got = swap_boundary(src.xch(), src.nslots(), epoch, src.slot_base() + u + 1, v);
                     pa.mine = v;
