@@ -4,8 +4,9 @@
 // each start to finish with no CTA-wide barrier:
 //
 //   1. lane 0 issues bulk async copies (cp.async.bulk through the TMA
-//      engine, L2 evict-first) of the tile's row_ptr window, col_idx slice
-//      and vals slice into one of the warp's STAGES shared-memory stages,
+//      engine, L2 evict-first) of the tile's row_ptr window (none for a
+//      tile inside one row), col_idx slice and vals slice into one of the
+//      warp's STAGES shared-memory stages,
 //      completing on that stage's mbarrier.  Ranges are rounded out to 16
 //      bytes (only the last few elements of an array, which rounding would
 //      overrun, are fetched with plain loads).  With STAGES = 2 the next
