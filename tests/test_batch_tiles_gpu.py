@@ -127,3 +127,30 @@ def test_matrix_tile_refused_on_warp_kernel_and_narrow_vectors():
 def test_matrix_tile_arguments_need_no_gpu():
     L = mb.lib()
     assert L.merbit_batch_set_matrix_tile(None, 0, 512, None) == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k,tile", [(2, 352), (4, 480), (8, 496), (16, 504), (32, 508)])
+def test_untuned_batch_defaults(k, tile):
+    """An untuned batch starts from the tile the tuner picks on the R-MAT
+    batch (staged products at k = 2, the odd tile of k at vector width 4);
+    with a leading dimension that rules out wide vectors it keeps 256."""
+    mats = _mats()[:5]
+    plans, Xs, Ys, xh = _operands(mats, k)
+    batch = mb.Batch(plans, Xs, Ys)
+    info = batch.info()
+    assert info["kernel"] == 0 and info["tile_items"] == tile
+    batch.run()
+    torch.cuda.synchronize()
+    for i, A in enumerate(mats):
+        if A.nrow:
+            yo, ya = O.spmm(A.row_ptr, A.col, A.vals.astype(np.float32), xh[i], k=k)
+            assert O.rel_error(Ys[i].cpu().numpy(), yo, ya)[0] <= 1e-6, (k, i)
+    batch.close()
+    # X with a leading dimension of k + 1: scalar loads only
+    Xw = [torch.zeros(A.ncol, k + 1, dtype=torch.float32, device="cuda") for A in mats]
+    for X, x in zip(Xw, xh):
+        X[:, :k] = torch.from_numpy(x).cuda()
+    b2 = mb.Batch(plans, [X[:, :k] for X in Xw], Ys)
+    assert b2.info()["tile_items"] == 256 and b2.info()["vector_width"] == 1
+    b2.close()
