@@ -633,8 +633,12 @@ def secondary_forms(args, A_zipf, rp, col, vals64, x64, dev, stream, peak,
 
     from merbit_b200 import synth
 
-    steps = args.steps
-    forms, ratios = {}, {}
+    # launches per measurement: up to 200 (one graph each); the batched
+    # form's plain FP64 side is 128 launches per step, so it takes up to 50
+    steps = min(args.steps, 200)
+    batch_steps = min(args.steps, 50)
+    forms, ratios = {"steps_per_measurement": steps,
+                     "steps_per_measurement_batched": batch_steps}, {}
     t0 = time.perf_counter()
     # precision form on the power-law matrix itself (same matrix, same k = 1)
     chk = not args.no_cpu_baseline
@@ -665,7 +669,7 @@ def secondary_forms(args, A_zipf, rp, col, vals64, x64, dev, stream, peak,
     del srp, scol, sv, sx, S
     torch.cuda.empty_cache()
     # batched form, k = 1 and 32
-    bf = batch_forms(steps, dev, stream, peak)
+    bf = batch_forms(batch_steps, dev, stream, peak)
     forms["rmat_batch128"] = bf
     torch.cuda.empty_cache()
     # differentiation form: Zipf(1.8) 1M rows, k = 16
