@@ -6,7 +6,8 @@ run through the configuration the tuner picks (the one the bench times):
   * Laplacian 256x256, FP64: against the oracle and against the reference
     merbit_kernel<double,256,14> run on this GPU (oracle/_ref);
   * Zipf(1.8) 2M rows, FP64: against the reference merbit_kernel (the
-    oracle comparison is in test_spmv_gpu.py);
+    oracle comparison is in test_spmv_gpu.py); FP32 and BF16 values with x
+    FP32: against the oracle on the stored inputs;
   * 27-point stencil 160^3 (4,096,000 rows, 109,215,352 nonzeros) with
     values stored FP64, FP32 and BF16 and x FP32: against the oracle on the
     stored inputs;
@@ -104,6 +105,19 @@ def test_zipf_2m_f64_vs_reference_kernel():
     yr = _reference_kernel_y(A, x)
     _, ya = O.spmm(A.row_ptr, A.col, A.vals, x)
     assert O.rel_error(y, yr, ya)[0] <= TOL_REF_KERNEL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_zipf_2m_precision_form_vs_oracle(dtype):
+    """The precision form on the headline matrix (values stored FP32/BF16,
+    x FP32): within 1e-6 of the FP64 oracle on the stored inputs."""
+    A = synth.workload("zipf_2m")
+    x = synth.workload_x("zipf_2m", A.ncol).astype(np.float32)
+    y = _tuned_spmv(A, dtype, x)
+    yo, ya = O.spmm(A.row_ptr, A.col, stored_values(A, dtype), x)
+    emax, emed = O.rel_error(y, yo, ya)
+    assert emax <= TOL[dtype], (emax, emed)
 
 
 @pytest.mark.gpu
